@@ -1,0 +1,370 @@
+"""Benchmark of le2d's time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 8192x8192 single solve (c1=3, c2=1.7, rho=2.5, h=1, dt=0.5*h/c1,
+8 seeded pressure disks), 1000 time steps per solve.  A bench "step" is one such
+solve (6.71e10 node-updates); the metric is node-updates/s (nu/s), one
+node-update = one node advanced one full time step (x- and y-sweep).
+
+Our arm (default) prints one JSON line with
+  value     nu/s with the state resident in HBM (CUDA events on the task's stream),
+  e2e       nu/s through the C ABI with host buffers: upload of the initial state
+            from page-locked memory, 1000 steps, download of the final fields,
+  roofline  the fused step kernel against the measured HBM copy bandwidth,
+            40 algorithmic bytes per node-update in FP32 (read + write of 5 fields),
+  cpu_baseline  the reference's own simple/ solver (oracle/_ref) on the host cores,
+  fp64      the same measurement for the FP64 library (80 B per node-update).
+Under torchrun each rank solves its own instance (independent solves, weak scaling);
+value is the total node-updates of all ranks over the slowest rank's time.
+
+--impl reference: the reference's own CPU solver (simple/ le_step, OpenMP over all
+host threads) on a bounded sample of the same workload (one time step per bench
+step); rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from le2d_b200 import capi, workloads  # noqa: E402
+
+BYTES_PER_NU = {"f": 40, "d": 80}
+SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return json.load(fh)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={SMI_FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def dist_init(world, local, backend):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def dist_max(dist, x: float, backend: str) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    dev = f"cuda:{torch.cuda.current_device()}" if backend == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def new_task(lib, p: workloads.Problem):
+    mat = lib.le_init_material(p.c1, p.c2, p.rho)
+    t = lib.le_init_task(p.dt, (p.hx, p.hy), mat, (p.nx, p.ny), capi.ST_AOS)
+    if not t.grid or lib.last_error(t):
+        raise RuntimeError(f"le_init_task failed: {lib.strerror(lib.last_error(t))}")
+    return t
+
+
+def initial_state(lib, p, t) -> np.ndarray:
+    """The workload's initial state (disks through le_set_ball) as a page-locked host copy."""
+    for cx, cy, r, s in p.disks:
+        lib.le_set_ball(t, (cx, cy), r, s)
+    assert lib.sync_host(t) == 0
+    return lib.grid_view(t)  # task->grid is page-locked
+
+
+def measure_ours(lib, prec, p, steps, warmup, dist, backend, device):
+    """Device-resident timing of `steps` solves and end-to-end timing through the C ABI."""
+    t = new_task(lib, p)
+    e2e_t = new_task(lib, p)
+    host_out, free_out = lib.host_array(5 * p.nodes)  # page-locked result buffer
+    try:
+        ic = initial_state(lib, p, t).copy()
+        host_in = lib.grid_view(e2e_t)  # page-locked input buffer (task->grid)
+        host_in[:] = ic
+        n = p.steps
+        # --- device-resident: K solves of n steps, state in HBM ---
+        for _ in range(warmup):
+            assert lib.upload(t, ic) == 0
+            rc, _ = lib.step_n_timed(t, n)
+            assert rc == 0, lib.strerror(rc)
+        assert lib.upload(t, ic) == 0 and lib.wait(t) == 0
+        dist_barrier(dist)
+        total_ms = 0.0
+        with ClockSampler(device) as clk:
+            for _ in range(steps):
+                rc, ms = lib.step_n_timed(t, n)  # events on the launching stream, synchronised
+                assert rc == 0, lib.strerror(rc)
+                total_ms += ms
+        dist_barrier(dist)
+        clocks = clk.summary()
+        slow_ms = dist_max(dist, total_ms, backend)
+        # --- end to end: upload from page-locked host memory, n steps, download ---
+        for _ in range(max(1, warmup // 2)):
+            assert lib.sync_device(e2e_t) == 0
+            assert lib.step_n(e2e_t, n) == 0 and lib.download(e2e_t, host_out) == 0
+        dist_barrier(dist)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            assert lib.sync_device(e2e_t) == 0       # H2D of task->grid (the initial state)
+            assert lib.step_n(e2e_t, n) == 0         # n time steps
+            assert lib.download(e2e_t, host_out) == 0  # D2H of the final fields, synchronised
+        e2e_s = time.perf_counter() - t0
+        dist_barrier(dist)
+        e2e_slow = dist_max(dist, e2e_s, backend)
+        assert np.isfinite(host_out).all()
+        return slow_ms, clocks, e2e_slow, ic
+    finally:
+        lib.le_free_task(t)
+        lib.le_free_task(e2e_t)
+        free_out()
+
+
+def cpu_reference_sample(p, budget_s=12.0):
+    """The reference simple/ solver (oracle/_ref) or, if absent, the C oracle port, timed on
+    all host threads over a bounded number of time steps of the same workload."""
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import ST_AOS, Oracle, Reference, ReferencePthread
+
+    threads = os.cpu_count() or 1
+    g = np.zeros(5 * p.nx * p.ny, np.float32)
+    o = Oracle("f")
+    for cx, cy, r, s in p.disks:
+        o.set_ball(g, p.nx, p.ny, p.hx, p.hy, ST_AOS, cx, cy, r, s)
+    out = {}
+    if Reference.available("f"):
+        ref = Reference("f")
+        t1 = ref.run(g.copy(), p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, ST_AOS, 1, threads)
+        k = max(1, min(20, int(budget_s / max(t1, 1e-3))))
+        tk = ref.run(g.copy(), p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, ST_AOS, k, threads)
+        out["simple"] = {"value": p.nx * p.ny * k / tk, "unit": "node-updates/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"reference simple/ le_step (gcc -O2 -fno-tree-vectorize, OpenMP), "
+                                   f"FP32, {p.nx}x{p.ny}, {k} time steps"}
+        if ReferencePthread.available("f"):
+            pt = ReferencePthread("f")
+            thr = max(1, min(threads, p.ny // 8))
+            t1 = pt.run(None, p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, 1, thr)
+            k = max(1, min(20, int(budget_s / max(t1, 1e-3))))
+            tk = pt.run(g.copy(), p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, k, thr)
+            out["pthread"] = {"value": p.nx * p.ny * k / tk, "unit": "node-updates/s", "cores": thr,
+                              "kind": "reference",
+                              "sample": f"reference pthread/ le_step (speed only), FP32, {p.nx}x{p.ny}, {k} steps"}
+    else:
+        t0 = time.perf_counter()
+        o.run(g, p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, ST_AOS, 1)
+        t1 = time.perf_counter() - t0
+        out["simple"] = {"value": p.nx * p.ny / t1, "unit": "node-updates/s", "cores": 1, "kind": "port",
+                         "sample": f"C oracle port (single thread), FP32, {p.nx}x{p.ny}, 1 time step"}
+    return out
+
+
+def run_reference_arm(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    from oracle.oracle import ST_AOS, Oracle, Reference
+
+    p = workloads.single_8192()
+    threads = os.cpu_count() or 1
+    g = np.zeros(5 * p.nx * p.ny, np.float32)
+    o = Oracle("f")
+    for cx, cy, r, s in p.disks:
+        o.set_ball(g, p.nx, p.ny, p.hx, p.hy, ST_AOS, cx, cy, r, s)
+    if Reference.available("f"):
+        runner = Reference("f")
+        kind = "reference"
+        step = lambda: runner.run(g, p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, ST_AOS, 1, threads)
+        sample = (f"reference simple/ le_step (oracle/_ref, gcc -O2 -fno-tree-vectorize, OpenMP {threads} threads), "
+                  f"FP32, one time step of {p.nx}x{p.ny} per bench step")
+    else:
+        kind = "port"
+        threads = 1
+
+        def step():
+            t0 = time.perf_counter()
+            o.run(g, p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, ST_AOS, 1)
+            return time.perf_counter() - t0
+
+        sample = f"C oracle port (single thread), FP32, one time step of {p.nx}x{p.ny} per bench step"
+    for _ in range(args.warmup):
+        step()
+    total = 0.0
+    for _ in range(args.steps):
+        total += step()
+    value = p.nx * p.ny * args.steps / total
+    line = {
+        "impl": "reference", "metric": "node-updates/s", "value": value, "unit": "node-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "single_8192 (one time step per bench step)", "nx": p.nx, "ny": p.ny,
+                   "parallelism": f"cpu{threads}"},
+        "cpu_baseline": {"value": value, "unit": "node-updates/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "node-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 leg")
+    ap.add_argument("--time-steps", type=int, default=None, help="time steps per solve (default 1000)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    world, rank, local = dist_setup()
+    backend = "nccl"
+    dist = dist_init(world, local, backend)
+    lib = capi.Lib("f")
+    assert lib.set_device(local) == 0
+    p = workloads.single_8192() if args.time_steps is None else workloads.single_8192(args.time_steps)
+    peak, peak_kind = measured_peaks()
+
+    slow_ms, clocks, e2e_s, ic = measure_ours(lib, "f", p, args.steps, args.warmup, dist, backend, local)
+    nu = p.node_updates * args.steps * world
+    value = nu / (slow_ms * 1e-3)
+    launches = args.steps * p.steps  # one fused-step kernel per time step
+    avg_launch_s = slow_ms * 1e-3 / launches
+    achieved = BYTES_PER_NU["f"] * p.nodes / avg_launch_s / 1e9
+    traffic = profiled_traffic().get("fused_step_f32_8192")
+    line = {
+        "metric": "node-updates/s", "value": value, "unit": "node-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": slow_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"single_8192: {p.nx}x{p.ny} grid, c1={p.c1}, c2={p.c2}, rho={p.rho}, "
+                               f"dt=0.5*h/c1, 8 seeded disks; one bench step = one solve of {p.steps} time steps",
+                   "nx": p.nx, "ny": p.ny, "time_steps_per_solve": p.steps,
+                   "l2": "state 1.34 GB (> 126 MB L2), no flush", "parallelism": f"independent solves x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind,
+                     "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                     "kernel": "fused_step_kernel<float,4>",
+                     "algorithmic_bytes_per_launch": BYTES_PER_NU["f"] * p.nodes},
+        "e2e": {"value": nu / e2e_s, "unit": "node-updates/s",
+                "h2d_bytes_per_step": int(ic.nbytes), "d2h_bytes_per_step": int(ic.nbytes)},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if not args.no_fp64:
+        libd = capi.Lib("d")
+        assert libd.set_device(local) == 0
+        ksteps = min(args.steps, 2)
+        d_ms, d_clk, d_e2e, d_ic = measure_ours(libd, "d", p, ksteps, min(args.warmup, 3), dist, backend, local)
+        d_nu = p.node_updates * ksteps * world
+        d_avg = d_ms * 1e-3 / (ksteps * p.steps)
+        d_ach = BYTES_PER_NU["d"] * p.nodes / d_avg / 1e9
+        line["fp64"] = {"value": d_nu / (d_ms * 1e-3), "unit": "node-updates/s", "steps": ksteps,
+                        "ms_per_step": d_ms / ksteps, "e2e": d_nu / d_e2e,
+                        "roofline": {"bound": "hbm", "achieved": d_ach, "peak": peak, "unit": "GB/s",
+                                     "frac": d_ach / peak, "kernel": "fused_step_kernel<double,2>"},
+                        "clocks": d_clk}
+    if rank == 0 and not args.no_cpu:
+        cb = cpu_reference_sample(p)
+        line["cpu_baseline"] = cb["simple"]
+        if "pthread" in cb:
+            line["cpu_baseline_pthread"] = cb["pthread"]
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,228 @@
+"""ctypes binding of the le2d C ABI (include/le_core.h, include/le2d.h).
+
+Mirrors the reference task API (le2d ``simple/le_core.h:217-254``) with the same
+names, argument meaning and struct layouts, for Python callers and the test
+suite.  ``Lib('f')`` binds lible2d_f.so (real = float), ``Lib('d')`` lible2d_d.so
+(real = double).  The library is the product path: if it is missing this module
+raises instead of computing anything itself.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(PKG, "lib")
+
+ST_SOA = 0
+ST_AOS = 1
+
+LE2D_OK = 0
+LE2D_EINVAL = 1
+LE2D_ENOTASK = 2
+LE2D_ESTYPE = 3
+LE2D_ECUDA = 4
+LE2D_ENOMEM = 5
+LE2D_ENODEV = 6
+LE2D_EBUDGET = 7
+LE2D_ETIMEOUT = 8
+LE2D_ESTATE = 9
+
+LE2D_METHOD_FUSED = 0
+LE2D_METHOD_SPLIT = 1
+
+# Every function the headers declare (checked by tests/test_abi.py).
+EXPORTS = [
+    "le_init_material", "le_init_task", "le_free_task", "le_set_ball", "le_save_task", "le_step",
+    "le_step_soa", "le2d_strerror", "le2d_set_device", "le2d_last_error", "le2d_clear_error", "le2d_sync_host",
+    "le2d_sync_device", "le2d_wait", "le2d_upload", "le2d_download", "le2d_step_n",
+    "le2d_step_n_timed", "le2d_set_method", "le2d_sim_time", "le2d_diagnostics",
+    "le2d_device_layout", "le2d_task_device_bytes", "le2d_host_alloc", "le2d_host_free",
+]
+
+
+class LibraryMissing(RuntimeError):
+    pass
+
+
+def lib_path(prec: str) -> str:
+    return os.path.join(LIBDIR, f"lible2d_{prec}.so")
+
+
+def _types(prec: str):
+    real = ctypes.c_float if prec == "f" else ctypes.c_double
+
+    class le_vec2(ctypes.Structure):
+        _fields_ = [("x", real), ("y", real)]
+
+    class le_point2(ctypes.Structure):
+        _fields_ = [("x", ctypes.c_int), ("y", ctypes.c_int)]
+
+    class le_material(ctypes.Structure):
+        _fields_ = [(n, real) for n in ("c1", "c2", "rho", "irhoc1", "irhoc2", "rhoc1", "rhoc2", "rhoc3")]
+
+    class le_task(ctypes.Structure):
+        _fields_ = [("dt", real), ("h", le_vec2), ("n", le_point2), ("mat", le_material),
+                    ("stype", ctypes.c_int), ("grid", ctypes.POINTER(real))]
+
+    class le2d_diag_t(ctypes.Structure):
+        _fields_ = [("energy", ctypes.c_double), ("sumsq", ctypes.c_double * 5),
+                    ("maxabs", ctypes.c_double * 5)]
+
+    return real, le_vec2, le_point2, le_material, le_task, le2d_diag_t
+
+
+class Lib:
+    """One precision of the library ('f' or 'd')."""
+
+    def __init__(self, prec: str = "f"):
+        path = lib_path(prec)
+        if not os.path.exists(path):
+            raise LibraryMissing(f"{path} is not built (python -m le2d_b200.build)")
+        self.prec = prec
+        self.dtype = np.float32 if prec == "f" else np.float64
+        self.lib = ctypes.CDLL(path)
+        (self.real, self.le_vec2, self.le_point2, self.le_material, self.le_task,
+         self.le2d_diag_t) = _types(prec)
+        L, R = self.lib, self.real
+        P = ctypes.POINTER
+        L.le_init_material.argtypes = [R, R, R, P(self.le_material)]
+        L.le_init_material.restype = None
+        L.le_init_task.argtypes = [P(self.le_task), R, self.le_vec2, self.le_material, self.le_point2,
+                                   ctypes.c_int]
+        L.le_init_task.restype = None
+        L.le_free_task.argtypes = [P(self.le_task)]
+        L.le_free_task.restype = None
+        L.le_set_ball.argtypes = [P(self.le_task), self.le_vec2, R, R]
+        L.le_set_ball.restype = None
+        L.le_save_task.argtypes = [P(self.le_task), ctypes.c_char_p]
+        L.le_step.argtypes = [P(self.le_task)]
+        L.le_step.restype = None
+        L.le_step_soa.argtypes = [P(self.le_task)]
+        L.le_step_soa.restype = None
+        L.le2d_strerror.argtypes = [ctypes.c_int]
+        L.le2d_strerror.restype = ctypes.c_char_p
+        L.le2d_set_device.argtypes = [ctypes.c_int]
+        for name in ("le2d_last_error", "le2d_clear_error", "le2d_sync_host", "le2d_sync_device",
+                     "le2d_wait"):
+            getattr(L, name).argtypes = [P(self.le_task)]
+        L.le2d_upload.argtypes = [P(self.le_task), ctypes.c_void_p]
+        L.le2d_download.argtypes = [P(self.le_task), ctypes.c_void_p]
+        L.le2d_step_n.argtypes = [P(self.le_task), ctypes.c_int]
+        L.le2d_step_n_timed.argtypes = [P(self.le_task), ctypes.c_int, P(ctypes.c_float)]
+        L.le2d_set_method.argtypes = [P(self.le_task), ctypes.c_int]
+        L.le2d_sim_time.argtypes = [P(self.le_task), P(ctypes.c_double), P(ctypes.c_longlong)]
+        L.le2d_diagnostics.argtypes = [P(self.le_task), P(self.le2d_diag_t)]
+        L.le2d_device_layout.argtypes = [P(self.le_task), P(ctypes.c_longlong), P(ctypes.c_longlong)]
+        L.le2d_task_device_bytes.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.le2d_task_device_bytes.restype = ctypes.c_size_t
+        L.le2d_host_alloc.argtypes = [ctypes.c_size_t]
+        L.le2d_host_alloc.restype = ctypes.c_void_p
+        L.le2d_host_free.argtypes = [ctypes.c_void_p]
+        L.le2d_host_free.restype = None
+
+    # --- the reference task API, same names ---
+    def le_init_material(self, c1, c2, rho):
+        m = self.le_material()
+        self.lib.le_init_material(c1, c2, rho, ctypes.byref(m))
+        return m
+
+    def le_init_task(self, dt, h, mat, n, stype):
+        t = self.le_task()
+        self.lib.le_init_task(ctypes.byref(t), dt, self.le_vec2(*h), mat, self.le_point2(*n), stype)
+        return t
+
+    def le_free_task(self, t):
+        self.lib.le_free_task(ctypes.byref(t))
+
+    def le_set_ball(self, t, c, r, s):
+        self.lib.le_set_ball(ctypes.byref(t), self.le_vec2(*c), r, s)
+
+    def le_save_task(self, t, path: str) -> int:
+        return self.lib.le_save_task(ctypes.byref(t), path.encode())
+
+    def le_step(self, t):
+        self.lib.le_step(ctypes.byref(t))
+
+    def le_step_soa(self, t):
+        self.lib.le_step_soa(ctypes.byref(t))
+
+    # --- extensions ---
+    def strerror(self, code: int) -> str:
+        return self.lib.le2d_strerror(code).decode()
+
+    def set_device(self, device: int) -> int:
+        return self.lib.le2d_set_device(device)
+
+    def last_error(self, t) -> int:
+        return self.lib.le2d_last_error(ctypes.byref(t))
+
+    def clear_error(self, t) -> int:
+        return self.lib.le2d_clear_error(ctypes.byref(t))
+
+    def sync_host(self, t) -> int:
+        return self.lib.le2d_sync_host(ctypes.byref(t))
+
+    def sync_device(self, t) -> int:
+        return self.lib.le2d_sync_device(ctypes.byref(t))
+
+    def wait(self, t) -> int:
+        return self.lib.le2d_wait(ctypes.byref(t))
+
+    def upload(self, t, src: np.ndarray) -> int:
+        assert src.dtype == self.dtype and src.flags["C_CONTIGUOUS"]
+        return self.lib.le2d_upload(ctypes.byref(t), src.ctypes.data)
+
+    def download(self, t, dst: np.ndarray) -> int:
+        assert dst.dtype == self.dtype and dst.flags["C_CONTIGUOUS"]
+        return self.lib.le2d_download(ctypes.byref(t), dst.ctypes.data)
+
+    def step_n(self, t, n: int) -> int:
+        return self.lib.le2d_step_n(ctypes.byref(t), n)
+
+    def step_n_timed(self, t, n: int):
+        ms = ctypes.c_float(0.0)
+        rc = self.lib.le2d_step_n_timed(ctypes.byref(t), n, ctypes.byref(ms))
+        return rc, ms.value
+
+    def set_method(self, t, method: int) -> int:
+        return self.lib.le2d_set_method(ctypes.byref(t), method)
+
+    def sim_time(self, t):
+        tt, st = ctypes.c_double(0.0), ctypes.c_longlong(0)
+        rc = self.lib.le2d_sim_time(ctypes.byref(t), ctypes.byref(tt), ctypes.byref(st))
+        return rc, tt.value, st.value
+
+    def diagnostics(self, t):
+        d = self.le2d_diag_t()
+        rc = self.lib.le2d_diagnostics(ctypes.byref(t), ctypes.byref(d))
+        return rc, {"energy": d.energy, "sumsq": list(d.sumsq), "maxabs": list(d.maxabs)}
+
+    def device_layout(self, t):
+        p, q = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        rc = self.lib.le2d_device_layout(ctypes.byref(t), ctypes.byref(p), ctypes.byref(q))
+        return rc, p.value, q.value
+
+    def task_device_bytes(self, nx: int, ny: int) -> int:
+        return self.lib.le2d_task_device_bytes(nx, ny)
+
+    def host_array(self, n: int):
+        """A page-locked numpy array of n reals and its release function."""
+        ptr = self.lib.le2d_host_alloc(n * np.dtype(self.dtype).itemsize)
+        if not ptr:
+            raise MemoryError("le2d_host_alloc failed")
+        buf = (self.real * n).from_address(ptr)
+        arr = np.ctypeslib.as_array(buf)
+        return arr, (lambda: self.lib.le2d_host_free(ptr))
+
+    # --- helpers ---
+    def grid_view(self, t) -> np.ndarray:
+        """The host grid (task->grid) as a numpy array (no copy)."""
+        n = 5 * t.n.x * t.n.y
+        return np.ctypeslib.as_array(t.grid, shape=(n,))
+
+
+def material_array(lib: Lib, m) -> np.ndarray:
+    return np.array([m.c1, m.c2, m.rho, m.irhoc1, m.irhoc2, m.rhoc1, m.rhoc2, m.rhoc3], dtype=lib.dtype)

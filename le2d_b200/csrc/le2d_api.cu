@@ -1,0 +1,622 @@
+// The le2d task API (include/le_core.h) and its extensions (include/le2d.h) on
+// one B200.  Compiled once per precision: `real` is float, or double with
+// -DUSE_DOUBLE (lible2d_f.so / lible2d_d.so), as the reference builds its
+// simple/ solver twice (simple/Makefile:6-7).
+//
+// State.  The reference keeps the grid in task->grid and steps it in place
+// (simple/le_core.c:605-620).  Here every task also owns a device state: two
+// pitched SoA buffers (ping-pong, since a step reads the old state while writing
+// the new one) registered under the task's grid pointer (the le_task struct has
+// no spare field and callers keep it on their stack, simple/main.c:27).  Steps
+// are queued on the task's stream and the host grid is refreshed only on
+// le_save_task, le2d_sync_host and le2d_download.
+//
+// Errors.  The reference asserts (simple/le_core.c:89, :261, :437); this library
+// never aborts or exits: it prints the cause on stderr and keeps the first error
+// per task (le2d_last_error).  There is no CPU fallback: without a device, steps
+// fail with LE2D_ENODEV.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+
+#include "le2d.h"
+#include "le2d_kernels.h"
+
+namespace {
+
+using T = real;
+using le2d::FusedPlan;
+using le2d::StepConsts;
+using le2d::Sweep;
+
+constexpr int kMinSeg = 16;  // shortest row segment of the fused kernel
+
+struct DevTask {
+  int nx = 0, ny = 0;
+  long long pitch = 0, plane = 0;
+  T* mem = nullptr;
+  T* buf[2] = {nullptr, nullptr};
+  int cur = 0;
+  double* d_diag = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  bool pinned = false;     // task->grid from cudaHostAlloc
+  bool host_newer = false; // task->grid holds a newer state than the device
+  bool dev_newer = false;  // the device holds a newer state than task->grid
+  bool has_device = false;
+  int err = LE2D_OK;
+  int method = LE2D_METHOD_FUSED;
+  FusedPlan plan;
+  long long steps = 0;
+  double sim_time = 0.0;
+  // CUDA graph of kGraphSteps steps starting from buffer graph_cur.
+  cudaGraphExec_t graph = nullptr;
+  int graph_cur = -1, graph_method = -1, graph_far_rot = -1;
+  StepConsts<T> graph_consts;
+};
+
+constexpr int kGraphSteps = 64;  // even, so a replay leaves the current buffer unchanged
+
+std::mutex g_mu;
+std::unordered_map<const void*, DevTask*> g_tasks;
+
+int device_count() {
+  static int n = -1;
+  if (n < 0) {
+    int c = 0;
+    n = cudaGetDeviceCount(&c) == cudaSuccess ? c : 0;
+    if (n == 0) cudaGetLastError();
+  }
+  return n;
+}
+
+int record(DevTask* d, int code, const char* what, cudaError_t e = cudaSuccess) {
+  if (e != cudaSuccess)
+    fprintf(stderr, "le2d: %s: %s\n", what, cudaGetErrorString(e));
+  else
+    fprintf(stderr, "le2d: %s: %s\n", what, le2d_strerror(code));
+  if (d && d->err == LE2D_OK) d->err = code;
+  return code;
+}
+
+DevTask* lookup(const le_task* task) {
+  if (!task || !task->grid) return nullptr;
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_tasks.find(task->grid);
+  return it == g_tasks.end() ? nullptr : it->second;
+}
+
+long long row_pitch(int nx) {
+  const int align = 128 / (int)sizeof(T);  // 128-byte rows
+  return ((long long)nx + align - 1) / align * align;
+}
+
+// Sweep constants of an axis with spacing h.  k1, k2 as the reference computes them,
+// in real (simple/le_core.c:468-469, :511-512); derived factors rounded once from double.
+Sweep<T> make_sweep(const le_task* t, T h) {
+  const T k1 = t->dt * t->mat.c1 / h;
+  const T k2 = t->dt * t->mat.c2 / h;
+  Sweep<T> s;
+  s.irhoc1 = t->mat.irhoc1;
+  s.irhoc2 = t->mat.irhoc2;
+  s.kc1 = (T)((1.0 - (double)k1) / 2.0);
+  s.kc2 = (T)((1.0 - (double)k2) / 2.0);
+  s.hk1 = (T)(0.5 * (double)k1);
+  s.hk2 = (T)(0.5 * (double)k2);
+  s.hk1rc1 = (T)(0.5 * (double)k1 * (double)t->mat.rhoc1);
+  s.hk1rc3 = (T)(0.5 * (double)k1 * (double)t->mat.rhoc3);
+  s.hk2rc2 = (T)(0.5 * (double)k2 * (double)t->mat.rhoc2);
+  s.k1 = k1;
+  s.k2 = k2;
+  s.rhoc1 = t->mat.rhoc1;
+  s.rhoc2 = t->mat.rhoc2;
+  s.rhoc3 = t->mat.rhoc3;
+  return s;
+}
+
+StepConsts<T> make_consts(const le_task* t) {
+  StepConsts<T> c;
+  c.x = make_sweep(t, t->h.x);
+  c.y = make_sweep(t, t->h.y);
+  return c;
+}
+
+bool same_consts(const StepConsts<T>& a, const StepConsts<T>& b) {
+  return memcmp(&a, &b, sizeof(a)) == 0;
+}
+
+int upload_raw(DevTask* d, const T* host, int aos) {
+  const size_t bytes = sizeof(T) * 5 * (size_t)d->nx * d->ny;
+  T* stage = d->buf[d->cur ^ 1];
+  cudaError_t e = cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, d->stream);
+  if (e != cudaSuccess) return record(d, LE2D_ECUDA, "upload", e);
+  e = le2d::launch_pack<T>(stage, d->buf[d->cur], d->nx, d->ny, d->pitch, d->plane, aos, d->stream);
+  if (e != cudaSuccess) return record(d, LE2D_ECUDA, "pack kernel", e);
+  return LE2D_OK;
+}
+
+int download_raw(DevTask* d, T* host, int aos) {
+  const size_t bytes = sizeof(T) * 5 * (size_t)d->nx * d->ny;
+  T* stage = d->buf[d->cur ^ 1];
+  cudaError_t e =
+      le2d::launch_unpack<T>(d->buf[d->cur], stage, d->nx, d->ny, d->pitch, d->plane, aos, d->stream);
+  if (e != cudaSuccess) return record(d, LE2D_ECUDA, "unpack kernel", e);
+  e = cudaMemcpyAsync(host, stage, bytes, cudaMemcpyDeviceToHost, d->stream);
+  if (e != cudaSuccess) return record(d, LE2D_ECUDA, "download", e);
+  e = cudaStreamSynchronize(d->stream);
+  if (e != cudaSuccess) return record(d, LE2D_ECUDA, "download sync", e);
+  return LE2D_OK;
+}
+
+int ensure_device_current(DevTask* d, le_task* task) {
+  if (!d->has_device) return record(d, LE2D_ENODEV, "no CUDA device");
+  if (d->host_newer) {
+    const int rc = upload_raw(d, task->grid, task->stype == ST_AOS);
+    if (rc) return rc;
+    d->host_newer = false;
+  }
+  return LE2D_OK;
+}
+
+int ensure_host_current(DevTask* d, le_task* task) {
+  if (d->dev_newer) {
+    const int rc = download_raw(d, task->grid, task->stype == ST_AOS);
+    if (rc) return rc;
+    d->dev_newer = false;
+  }
+  return LE2D_OK;
+}
+
+// Queues one step from buf[cur]; the fused kernel writes buf[cur^1] and flips cur,
+// the split scheme sweeps x into buf[cur^1] and y back into buf[cur].
+cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int method, int* cur) {
+  T* a = d->buf[*cur];
+  T* b = d->buf[*cur ^ 1];
+  if (method == LE2D_METHOD_SPLIT) {
+    cudaError_t e = le2d::launch_split_sweep<T>(0, a, b, d->nx, d->ny, d->pitch, d->plane, c.x,
+                                                c.x.k1, c.x.k2, 0, d->stream);
+    if (e != cudaSuccess) return e;
+    return le2d::launch_split_sweep<T>(1, b, a, d->nx, d->ny, d->pitch, d->plane, c.y, c.y.k1,
+                                       c.y.k2, far_rot, d->stream);
+  }
+  cudaError_t e = le2d::launch_fused_step<T>(a, b, d->nx, d->ny, d->pitch, d->plane, c, far_rot,
+                                             d->plan, d->stream);
+  *cur ^= 1;
+  return e;
+}
+
+int run_steps(le_task* task, int nsteps, bool soa_entry, float* ms) {
+  DevTask* d = lookup(task);
+  if (!d) {
+    fprintf(stderr, "le2d: step: task was not created by le_init_task\n");
+    return LE2D_ENOTASK;
+  }
+  if (nsteps < 0) return record(d, LE2D_EINVAL, "step count < 0");
+  if (soa_entry ? task->stype != ST_SOA : task->stype != ST_AOS)
+    return record(d, LE2D_ESTYPE, soa_entry ? "le_step_soa needs an ST_SOA task"
+                                            : "le_step needs an ST_AOS task");
+  if (d->nx < 3 || d->ny < 3) return record(d, LE2D_EINVAL, "step: the scheme needs n.x, n.y >= 3");
+  int rc = ensure_device_current(d, task);
+  if (rc) return rc;
+  const StepConsts<T> c = make_consts(task);
+  const int far_rot = soa_entry ? 1 : 0;
+  cudaError_t e = cudaSuccess;
+  if (ms) {
+    e = cudaEventRecord(d->ev[0], d->stream);
+    if (e != cudaSuccess) return record(d, LE2D_ECUDA, "event record", e);
+  }
+  int left = nsteps;
+  // Long runs replay a captured graph of kGraphSteps steps (even count: buffers end where
+  // they started).
+  while (left >= kGraphSteps) {
+    const bool valid = d->graph && d->graph_cur == d->cur && d->graph_method == d->method &&
+                       d->graph_far_rot == far_rot && same_consts(d->graph_consts, c);
+    if (!valid) {
+      if (d->graph) cudaGraphExecDestroy(d->graph);
+      d->graph = nullptr;
+      cudaGraph_t g = nullptr;
+      e = cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return record(d, LE2D_ECUDA, "graph capture", e);
+      int cur = d->cur;
+      for (int s = 0; s < kGraphSteps && e == cudaSuccess; ++s) e = queue_step(d, c, far_rot, d->method, &cur);
+      cudaError_t e2 = cudaStreamEndCapture(d->stream, &g);
+      if (e != cudaSuccess || e2 != cudaSuccess)
+        return record(d, LE2D_ECUDA, "graph capture", e != cudaSuccess ? e : e2);
+      e = cudaGraphInstantiate(&d->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return record(d, LE2D_ECUDA, "graph instantiate", e);
+      d->graph_cur = d->cur;
+      d->graph_method = d->method;
+      d->graph_far_rot = far_rot;
+      d->graph_consts = c;
+    }
+    e = cudaGraphLaunch(d->graph, d->stream);
+    if (e != cudaSuccess) return record(d, LE2D_ECUDA, "graph launch", e);
+    left -= kGraphSteps;
+  }
+  for (; left > 0; --left) {
+    e = queue_step(d, c, far_rot, d->method, &d->cur);
+    if (e != cudaSuccess) return record(d, LE2D_ECUDA, "step kernel launch", e);
+  }
+  if (ms) {
+    e = cudaEventRecord(d->ev[1], d->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(d->ev[1]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, d->ev[0], d->ev[1]);
+    if (e != cudaSuccess) return record(d, LE2D_ECUDA, "step timing", e);
+  }
+  // FP64 simulated-time accumulator: one dt per step.
+  for (int s = 0; s < nsteps; ++s) d->sim_time += (double)task->dt;
+  d->steps += nsteps;
+  if (nsteps > 0) d->dev_newer = true;
+  return LE2D_OK;
+}
+
+void release(DevTask* d) {
+  if (d->graph) cudaGraphExecDestroy(d->graph);
+  if (d->ev[0]) cudaEventDestroy(d->ev[0]);
+  if (d->ev[1]) cudaEventDestroy(d->ev[1]);
+  if (d->stream) {
+    cudaStreamSynchronize(d->stream);
+    cudaStreamDestroy(d->stream);
+  }
+  if (d->mem) cudaFree(d->mem);
+  if (d->d_diag) cudaFree(d->d_diag);
+  delete d;
+}
+
+// Host le_set_ball loop: position h*i in real, squared distance in real, sqrt and the
+// test against r in double, overwrite sxx and syy (simple/le_core.c:71-94).
+void set_ball_host(le_task* t, const le_vec2 c, const real r, const real s) {
+  const long long plane = (long long)t->n.x * t->n.y;
+  for (int i = 0; i < t->n.x; i++) {
+    for (int j = 0; j < t->n.y; j++) {
+      const real px = t->h.x * i;
+      const real py = t->h.y * j;
+      const real dx = px - c.x;
+      const real dy = py - c.y;
+      if (sqrt(dx * dx + dy * dy) < r) {
+        const long long q = i + (long long)j * t->n.x;
+        if (t->stype == ST_AOS) {
+          t->grid[q * 5 + 2] = s;
+          t->grid[q * 5 + 4] = s;
+        } else {
+          t->grid[2 * plane + q] = s;
+          t->grid[4 * plane + q] = s;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* le2d_strerror(int code) {
+  switch (code) {
+    case LE2D_OK: return "ok";
+    case LE2D_EINVAL: return "invalid argument";
+    case LE2D_ENOTASK: return "task not created by le_init_task";
+    case LE2D_ESTYPE: return "wrong storage type for this step function";
+    case LE2D_ECUDA: return "CUDA error";
+    case LE2D_ENOMEM: return "out of memory";
+    case LE2D_ENODEV: return "no CUDA device";
+    case LE2D_EBUDGET: return "exceeds the HBM budget";
+    case LE2D_ETIMEOUT: return "device wait timed out";
+    case LE2D_ESTATE: return "not allowed in the current state";
+    default: return "unknown error";
+  }
+}
+
+int le2d_set_device(int device) {
+  if (device < 0 || device >= device_count()) return LE2D_ENODEV;
+  cudaError_t e = cudaSetDevice(device);
+  return e == cudaSuccess ? LE2D_OK : record(nullptr, LE2D_ECUDA, "le2d_set_device", e);
+}
+
+// simple/le_core.c:171-187, same expressions and type promotions.
+void le_init_material(const real c1, const real c2, const real rho, le_material* m) {
+  m->c1 = c1;
+  m->c2 = c2;
+  m->rho = rho;
+  m->irhoc1 = 1.0 / (c1 * rho);
+  m->irhoc2 = 1.0 / (c2 * rho);
+  m->rhoc1 = c1 * rho;
+  m->rhoc2 = c2 * rho;
+  const real mu = rho * c2 * c2;
+  const real la = rho * c1 * c1 - 2.0 * mu;
+  m->rhoc3 = rho * c1 * la / (la + 2.0 * mu);
+}
+
+size_t le2d_task_device_bytes(int nx, int ny) {
+  if (nx < 1 || ny < 1) return 0;
+  return sizeof(T) * 2 * 5 * (size_t)row_pitch(nx) * (size_t)ny + 16 * sizeof(double);
+}
+
+void le_init_task(le_task* task, const real dt, const le_vec2 h, const le_material mat,
+                  const le_point2 n, const int stype) {
+  task->dt = dt;
+  task->h = h;
+  task->mat = mat;
+  task->n = n;
+  task->stype = stype;
+  task->grid = nullptr;
+  if (n.x < 1 || n.y < 1) {
+    fprintf(stderr, "le2d: le_init_task: bad grid size %d x %d\n", n.x, n.y);
+    return;
+  }
+  const size_t bytes = sizeof(le_node) * (size_t)n.x * n.y;
+  DevTask* d = new DevTask();
+  d->nx = n.x;
+  d->ny = n.y;
+  d->has_device = device_count() > 0;
+  void* hp = nullptr;
+  if (d->has_device && cudaHostAlloc(&hp, bytes, cudaHostAllocDefault) == cudaSuccess) {
+    d->pinned = true;
+  } else {
+    if (d->has_device) cudaGetLastError();
+    hp = malloc(bytes);
+  }
+  if (!hp) {
+    fprintf(stderr, "le2d: le_init_task: host allocation of %zu bytes failed\n", bytes);
+    delete d;
+    return;
+  }
+  memset(hp, 0, bytes);
+  task->grid = (real*)hp;
+  if (n.x < 3 || n.y < 3) record(d, LE2D_EINVAL, "le_init_task: the scheme needs n.x, n.y >= 3");
+  if (stype != ST_AOS && stype != ST_SOA) record(d, LE2D_EINVAL, "le_init_task: unknown stype");
+  if (d->has_device) {
+    d->pitch = row_pitch(n.x);
+    d->plane = d->pitch * n.y;
+    const size_t dbytes = sizeof(T) * 2 * 5 * (size_t)d->plane;
+    cudaError_t e = cudaMalloc(&d->mem, dbytes);
+    if (e != cudaSuccess) {
+      record(d, LE2D_ENOMEM, "le_init_task: device state", e);
+      d->mem = nullptr;
+      d->has_device = false;
+    } else {
+      d->buf[0] = d->mem;
+      d->buf[1] = d->mem + 5 * d->plane;
+      e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreate(&d->ev[0]);
+      if (e == cudaSuccess) e = cudaEventCreate(&d->ev[1]);
+      if (e == cudaSuccess) e = cudaMalloc(&d->d_diag, 16 * sizeof(double));
+      if (e == cudaSuccess) e = cudaMemsetAsync(d->mem, 0, dbytes, d->stream);
+      if (e != cudaSuccess) {
+        record(d, LE2D_ECUDA, "le_init_task: device setup", e);
+        d->has_device = false;
+      }
+      int dev = 0;
+      cudaGetDevice(&dev);
+      d->plan = le2d::plan_fused<T>(n.x, n.y, le2d::fused_resident_warps<T>(dev), kMinSeg);
+    }
+  } else {
+    record(d, LE2D_ENODEV, "le_init_task");
+  }
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_tasks[task->grid] = d;
+}
+
+void le_free_task(le_task* task) {
+  if (!task || !task->grid) return;
+  DevTask* d = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_tasks.find(task->grid);
+    if (it != g_tasks.end()) {
+      d = it->second;
+      g_tasks.erase(it);
+    }
+  }
+  const bool pinned = d && d->pinned;
+  if (d) release(d);
+  if (pinned)
+    cudaFreeHost(task->grid);
+  else
+    free(task->grid);
+  task->grid = nullptr;
+}
+
+void le_set_ball(le_task* t, const le_vec2 c, const real r, const real s) {
+  DevTask* d = lookup(t);
+  if (t->stype != ST_AOS && t->stype != ST_SOA) {
+    record(d, LE2D_EINVAL, "le_set_ball: unknown stype");
+    return;
+  }
+  if (d && d->has_device && !d->host_newer) {
+    cudaError_t e = le2d::launch_set_ball<T>(d->buf[d->cur], d->nx, d->ny, d->pitch, d->plane,
+                                             t->h.x, t->h.y, c.x, c.y, r, s, d->stream);
+    if (e != cudaSuccess) {
+      record(d, LE2D_ECUDA, "le_set_ball kernel", e);
+      return;
+    }
+    d->dev_newer = true;
+    return;
+  }
+  if (d && d->dev_newer && ensure_host_current(d, t)) return;
+  set_ball_host(t, c, r, s);
+  if (d) d->host_newer = true;
+}
+
+// simple/le_core.c:130-169 with write_float :99-111: header, then |v| as big-endian float32.
+int le_save_task(le_task* t, const char* file) {
+  DevTask* d = lookup(t);
+  if (d && ensure_host_current(d, t)) return 1;
+  FILE* fp = fopen(file, "w");
+  if (!fp) {
+    perror("Failed to open file");
+    return 1;
+  }
+  fprintf(fp, "# vtk DataFile Version 3.0\n");
+  fprintf(fp, "Created by le_save_task\n");
+  fprintf(fp, "BINARY\n");
+  fprintf(fp, "DATASET STRUCTURED_POINTS\n");
+  fprintf(fp, "DIMENSIONS %d %d 1\n", t->n.x, t->n.y);
+  fprintf(fp, "SPACING %f %f 0.0\n", t->h.x, t->h.y);
+  fprintf(fp, "ORIGIN 0.0 0.0 0.0\n");
+  fprintf(fp, "POINT_DATA %d\n", t->n.x * t->n.y);
+  fprintf(fp, "SCALARS v float 1\n");
+  fprintf(fp, "LOOKUP_TABLE v_table\n");
+  const long long plane = (long long)t->n.x * t->n.y;
+  const int nx = t->n.x;
+  unsigned char* row = (unsigned char*)malloc(4 * (size_t)nx);
+  for (int j = 0; j < t->n.y && row; j++) {
+    for (int i = 0; i < nx; i++) {
+      const long long q = i + (long long)j * nx;
+      const real vx = t->stype == ST_AOS ? t->grid[q * 5 + 0] : t->grid[q];
+      const real vy = t->stype == ST_AOS ? t->grid[q * 5 + 1] : t->grid[plane + q];
+      const float v = sqrt(vx * vx + vy * vy);
+      unsigned char b[4];
+      memcpy(b, &v, 4);
+      row[4 * i + 0] = b[3];
+      row[4 * i + 1] = b[2];
+      row[4 * i + 2] = b[1];
+      row[4 * i + 3] = b[0];
+    }
+    fwrite(row, 1, 4 * (size_t)nx, fp);
+  }
+  free(row);
+  fclose(fp);
+  return 0;
+}
+
+void le_step(le_task* task) { run_steps(task, 1, false, nullptr); }
+
+void le_step_soa(le_task* task) { run_steps(task, 1, true, nullptr); }
+
+int le2d_step_n(le_task* task, int nsteps) {
+  return run_steps(task, nsteps, task && task->stype == ST_SOA, nullptr);
+}
+
+int le2d_step_n_timed(le_task* task, int nsteps, float* ms) {
+  if (!ms) return LE2D_EINVAL;
+  return run_steps(task, nsteps, task && task->stype == ST_SOA, ms);
+}
+
+int le2d_last_error(const le_task* task) {
+  DevTask* d = lookup(task);
+  return d ? d->err : LE2D_ENOTASK;
+}
+
+int le2d_clear_error(le_task* task) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  d->err = LE2D_OK;
+  return LE2D_OK;
+}
+
+int le2d_sync_host(le_task* task) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  return ensure_host_current(d, task);
+}
+
+int le2d_sync_device(le_task* task) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  d->host_newer = true;
+  d->dev_newer = false;
+  return ensure_device_current(d, task);
+}
+
+int le2d_upload(le_task* task, const real* src) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  if (!src) return record(d, LE2D_EINVAL, "le2d_upload: NULL source");
+  if (!d->has_device) return record(d, LE2D_ENODEV, "le2d_upload");
+  const int rc = upload_raw(d, src, task->stype == ST_AOS);
+  if (rc) return rc;
+  d->host_newer = false;
+  d->dev_newer = true;
+  return LE2D_OK;
+}
+
+int le2d_download(le_task* task, real* dst) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  if (!dst) return record(d, LE2D_EINVAL, "le2d_download: NULL destination");
+  if (d->host_newer) {
+    memcpy(dst, task->grid, sizeof(le_node) * (size_t)d->nx * d->ny);
+    return LE2D_OK;
+  }
+  if (!d->has_device) return record(d, LE2D_ENODEV, "le2d_download");
+  return download_raw(d, dst, task->stype == ST_AOS);
+}
+
+void* le2d_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (device_count() == 0 || cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void le2d_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+int le2d_wait(le_task* task) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  if (!d->has_device) return LE2D_OK;
+  cudaError_t e = cudaStreamSynchronize(d->stream);
+  return e == cudaSuccess ? LE2D_OK : record(d, LE2D_ECUDA, "wait", e);
+}
+
+int le2d_set_method(le_task* task, int method) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  if (method != LE2D_METHOD_FUSED && method != LE2D_METHOD_SPLIT) return LE2D_EINVAL;
+  d->method = method;
+  return LE2D_OK;
+}
+
+int le2d_sim_time(const le_task* task, double* t, long long* steps) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  if (t) *t = d->sim_time;
+  if (steps) *steps = d->steps;
+  return LE2D_OK;
+}
+
+int le2d_diagnostics(le_task* task, le2d_diag_t* out) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  if (!out) return LE2D_EINVAL;
+  int rc = ensure_device_current(d, task);
+  if (rc) return rc;
+  const double rho = task->mat.rho, c1 = task->mat.c1, c2 = task->mat.c2;
+  const double mu = rho * c2 * c2, la = rho * c1 * c1 - 2.0 * mu;
+  const double a_nn = (la + 2.0 * mu) / (8.0 * mu * (la + mu));
+  const double a_xy = -2.0 * la / (8.0 * mu * (la + mu));
+  const double a_s = 1.0 / (2.0 * mu);
+  double h[11];
+  cudaError_t e = cudaMemsetAsync(d->d_diag, 0, 11 * sizeof(double), d->stream);
+  if (e == cudaSuccess)
+    e = le2d::launch_diag<T>(d->buf[d->cur], d->nx, d->ny, d->pitch, d->plane, rho, a_nn, a_xy, a_s,
+                             d->d_diag, d->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, d->d_diag, sizeof(h), cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  if (e != cudaSuccess) return record(d, LE2D_ECUDA, "diagnostics", e);
+  out->energy = h[0] * (double)task->h.x * (double)task->h.y;
+  for (int k = 0; k < 5; ++k) {
+    out->sumsq[k] = h[1 + k];
+    out->maxabs[k] = h[6 + k];
+  }
+  return LE2D_OK;
+}
+
+int le2d_device_layout(const le_task* task, long long* pitch_elems, long long* plane_elems) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  if (pitch_elems) *pitch_elems = d->pitch;
+  if (plane_elems) *plane_elems = d->plane;
+  return LE2D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+// Device-side math of le2d's grid-characteristic step, shared by every kernel.
+//
+// One time step (le2d simple/le_core.c:605-620) is an x-sweep then a y-sweep.  A
+// sweep along axis a maps the five fields of each node to four moving Riemann
+// invariants (omega, simple/le_core.c:192-218), transports each with the
+// second-order superbee-limited upwind scheme (tvd2, :48-69) and maps the change
+// back to the fields (inc_x / inc_y, :221-249).
+//
+// Face form.  tvd2's slope ratio "r_1" at node i is the ratio "r" of node i-1, and
+// its flux "f_12" at node i is the flux "f12" of node i-1 (same operands, same
+// operations).  So the kernels compute one ratio and one limited flux per face and
+// share it between the two nodes that touch the face:
+//   right-moving invariant u (w1, w3):  D_i = u_{i+1} - u_i, P_i = D_i + eps,
+//       F_i = u_i + psi(P_{i-1} / P_i) D_i,          new u_i = u_i - k (F_i - F_{i-1})
+//   left-moving invariant u (w2, w4):   Q_i = eps - D_i,
+//       G_i = u_i - psi(Q_i / Q_{i-1}) D_{i-1},      new u_i = u_i - k (G_i - G_{i+1})
+// with psi(r) = (1 - k)/2 * superbee(r).  The field update uses the invariant
+// changes directly, 0.5*(new u - u) = k/2 (F_{i-1} - F_i), instead of forming
+// new u and subtracting u again.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace le2d {
+
+enum Field { VX = 0, VY = 1, SXX = 2, SXY = 3, SYY = 4, NF = 5 };
+
+// Constants of one directional sweep (built on the host by make_sweep()).
+template <typename T>
+struct Sweep {
+  T irhoc1, irhoc2;          // omega: w = v -+ s * irhoc
+  T kc1, kc2;                // (1 - k)/2 for the P (k1) and S (k2) Courant numbers
+  T hk1, hk2;                // k/2
+  T hk1rc1, hk1rc3, hk2rc2;  // k1/2 * rhoc1, k1/2 * rhoc3, k2/2 * rhoc2
+  T k1, k2;                  // Courant numbers dt*c/h (plain per-node scheme)
+  T rhoc1, rhoc2, rhoc3;     // the material's products (plain per-node scheme)
+};
+
+template <typename T>
+struct StepConsts {
+  Sweep<T> x, y;
+};
+
+template <typename T>
+__device__ __forceinline__ T tvd_eps();
+template <>
+__device__ __forceinline__ float tvd_eps<float>() { return 1e-6f; }  // TVD2_EPS, simple/le_core.c:29
+template <>
+__device__ __forceinline__ double tvd_eps<double>() { return 1e-6; }
+
+// Slope ratio a / b.  FP32: hardware reciprocal (rcp.approx, <= 1 ulp) times a;
+// for b = +-0 it gives +-inf (a != 0) or NaN (a = 0) like the division does, and the
+// limiter maps those exactly as the reference (superbee(+-inf) = 2 / 0, superbee(NaN) = 2).
+// FP64: IEEE division.
+__device__ __forceinline__ float ratio(float a, float b) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+  return a * r;
+}
+__device__ __forceinline__ double ratio(double a, double b) { return a / b; }
+
+__device__ __forceinline__ float max3(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+__device__ __forceinline__ double max3(double a, double b, double c) { return fmax(a, fmax(b, c)); }
+
+// kc * superbee(r), superbee(r) = max(0, min(1, 2r), min(2, r))  (simple/le_core.c:38).
+// fmin returns the non-NaN operand, so superbee(NaN) = max(0, 1, 2) = 2 as in le_min/le_max.
+template <typename T>
+__device__ __forceinline__ T psi(T r, T kc) {
+  return kc * max3(T(0), fmin(T(1), r + r), fmin(T(2), r));
+}
+
+// Limited flux of a right-moving invariant through the face right of node i.
+template <typename T>
+__device__ __forceinline__ T flux_fwd(T u, T p_left, T p_right, T d_right, T kc) {
+  return fma(psi(ratio(p_left, p_right), kc), d_right, u);
+}
+
+// Limited flux of a left-moving invariant through the face left of node i.
+template <typename T>
+__device__ __forceinline__ T flux_bwd(T u, T q_left, T q_right, T d_left, T kc) {
+  return fma(-psi(ratio(q_right, q_left), kc), d_left, u);
+}
+
+// Invariants of one node for a sweep along AXIS (0 = x, 1 = y).
+template <int AXIS, typename T>
+__device__ __forceinline__ void omega(T vx, T vy, T sxx, T sxy, T syy, const Sweep<T>& c, T& w1,
+                                      T& w2, T& w3, T& w4) {
+  const T vn = AXIS == 0 ? vx : vy;
+  const T vt = AXIS == 0 ? vy : vx;
+  const T sn = AXIS == 0 ? sxx : syy;
+  const T n00 = sn * c.irhoc1;
+  const T n01 = sxy * c.irhoc2;
+  w1 = vn - n00;
+  w2 = vn + n00;
+  w3 = vt - n01;
+  w4 = vt + n01;
+}
+
+// Field update of one node from the flux differences of its four invariants:
+// a1 = F1_{i-1} - F1_i, b2 = G2_{i+1} - G2_i, a3, b4 likewise (inc_x / inc_y).
+template <int AXIS, typename T>
+__device__ __forceinline__ void apply_increment(T& vx, T& vy, T& sxx, T& sxy, T& syy, T a1, T b2,
+                                                T a3, T b4, const Sweep<T>& c) {
+  T& vn = AXIS == 0 ? vx : vy;
+  T& vt = AXIS == 0 ? vy : vx;
+  T& sn = AXIS == 0 ? sxx : syy;
+  T& so = AXIS == 0 ? syy : sxx;
+  const T p = b2 - a1;
+  vn = fma(c.hk1, a1 + b2, vn);
+  vt = fma(c.hk2, a3 + b4, vt);
+  sn = fma(c.hk1rc1, p, sn);
+  so = fma(c.hk1rc3, p, so);
+  sxy = fma(c.hk2rc2, b4 - a3, sxy);
+}
+
+}  // namespace le2d

@@ -1,0 +1,253 @@
+"""Parity of the CUDA path with the reference, through the C ABI.
+
+Tolerances (per field, relative L2 = ||a-b|| / ||b||):
+  * FP64 library vs the reference double build: <= 1e-12
+  * FP32 library vs the reference float build:  <= 1e-5, and vs the double build too.
+    Where a field's norm is tiny next to the others (e.g. noise-level vx beside unit
+    stresses on a 3x7 grid) one float ulp of the large fields is already ~1e-4 of the
+    small field's norm, and the reference's own float build sits up to 3e-5 from its
+    double build; for such a field the bound is 4x the reference float build's own
+    distance from its double build when that exceeds 1e-5/4.
+Max-abs error of every result against the FP64 reference is printed (pytest -s).
+"""
+import numpy as np
+import pytest
+
+from golden_cases import arrays, cases
+from le2d_b200 import capi, workloads
+from oracle.oracle import ST_AOS, ST_SOA, Oracle, aos_to_soa, fields, max_abs, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"d": 1e-12, "f": 1e-5}
+METHODS = {"fused": capi.LE2D_METHOD_FUSED, "split": capi.LE2D_METHOD_SPLIT}
+
+
+@pytest.fixture(scope="module")
+def libs():
+    return {p: capi.Lib(p) for p in ("f", "d")}
+
+
+def make_task(lib, c, method=capi.LE2D_METHOD_FUSED):
+    mat = lib.le_init_material(c["c1"], c["c2"], c["rho"])
+    t = lib.le_init_task(c["dt"], (c["hx"], c["hy"]), mat, (c["nx"], c["ny"]), c["stype"])
+    assert t.grid
+    assert lib.set_method(t, method) == 0
+    return t
+
+
+def run(lib, c, g0, steps, method=capi.LE2D_METHOD_FUSED, per_call=True):
+    """Steps a copy of g0 through the library; returns the final grid (task layout)."""
+    t = make_task(lib, c, method)
+    try:
+        assert lib.upload(t, np.ascontiguousarray(g0, dtype=lib.dtype)) == 0
+        if per_call:
+            step = lib.le_step if c["stype"] == ST_AOS else lib.le_step_soa
+            for _ in range(steps):
+                step(t)
+        else:
+            assert lib.step_n(t, steps) == 0
+        out = np.zeros(5 * c["nx"] * c["ny"], lib.dtype)
+        assert lib.download(t, out) == 0
+        assert lib.last_error(t) == 0, lib.strerror(lib.last_error(t))
+        return out
+    finally:
+        lib.le_free_task(t)
+
+
+def fp32_tolerance(want_f, want_d):
+    """Per-field FP32 bound: 1e-5, or 4x the reference float build's distance from its
+    double build where that distance exceeds 1e-5/4."""
+    gap = rel_l2(want_f, want_d)
+    return np.maximum(TOL["f"], 4.0 * gap)
+
+
+def check(prec, got, want, want_d, nx, ny, stype, label):
+    g = fields(got, nx, ny, stype)
+    w = fields(want, nx, ny, stype)
+    wd = fields(want_d, nx, ny, stype)
+    err = rel_l2(g, w)
+    mab = max_abs(g, wd)
+    print(f"\n{label}: rel_l2={np.array2string(err, precision=2)} max_abs_vs_fp64={np.array2string(mab, precision=2)}")
+    if prec == "d":
+        assert np.all(err <= TOL["d"]), (label, err)
+    else:
+        tol = fp32_tolerance(w, wd)
+        assert np.all(err <= tol), (label, err, tol)
+        assert np.all(rel_l2(g, wd) <= tol), (label, rel_l2(g, wd), tol)
+
+
+@pytest.mark.parametrize("method", sorted(METHODS))
+@pytest.mark.parametrize("prec", ["f", "d"])
+@pytest.mark.parametrize("name", sorted(cases()))
+def test_golden_case(libs, name, prec, method):
+    c = cases()[name]
+    a, ad = arrays(prec), arrays("d")
+    got = run(libs[prec], c, a[f"{name}__in"], c["steps"], METHODS[method])
+    check(prec, got, a[f"{name}__out"], ad[f"{name}__out"], c["nx"], c["ny"], c["stype"],
+          f"{name}/{prec}/{method}")
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_set_ball_device_bitwise(libs, prec):
+    """le_set_ball on the device reproduces the reference initial condition bit for bit."""
+    lib = libs[prec]
+    o = Oracle(prec)
+    for name in ("disks_noise_37x53", "strips_250x40", "soa_40x32"):
+        c = cases()[name]
+        t = make_task(lib, c)
+        try:
+            for cx, cy, r, s in c["disks"]:
+                lib.le_set_ball(t, (cx, cy), r, s)
+            assert lib.sync_host(t) == 0
+            got = lib.grid_view(t).copy()
+        finally:
+            lib.le_free_task(t)
+        want = np.zeros_like(got)
+        for d in c["disks"]:
+            o.set_ball(want, c["nx"], c["ny"], c["hx"], c["hy"], c["stype"], *d)
+        assert got.tobytes() == want.tobytes(), name
+
+
+def _medium(prec, stype, nx=300, ny=200, steps=150):
+    rng = np.random.default_rng(7)
+    p = dict(nx=nx, ny=ny, hx=1.0, hy=0.8, c1=2.5, c2=1.2, rho=1.7, stype=stype)
+    p["dt"] = 0.45 * 0.8 / 2.5
+    o = Oracle(prec)
+    g0 = np.zeros(5 * nx * ny, o.dtype)
+    for _ in range(5):
+        o.set_ball(g0, nx, ny, 1.0, 0.8, stype, float(rng.uniform(0, nx)), float(rng.uniform(0, ny * 0.8)),
+                   float(rng.uniform(5, 40)), float(rng.uniform(-2, 2)))
+    g0 += rng.uniform(-1e-3, 1e-3, size=g0.shape).astype(o.dtype)
+    return p, g0, steps
+
+
+@pytest.mark.parametrize("method", sorted(METHODS))
+@pytest.mark.parametrize("stype", [ST_AOS, ST_SOA])
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_oracle_medium(libs, prec, stype, method):
+    """300x200, five disks + noise, 150 steps (waves cross every boundary), vs the oracle."""
+    p, g0, steps = _medium(prec, stype)
+    want = g0.copy()
+    Oracle(prec).run(want, p["nx"], p["ny"], p["dt"], p["hx"], p["hy"], p["c1"], p["c2"], p["rho"], stype, steps)
+    gd = g0.astype(np.float64)
+    Oracle("d").run(gd, p["nx"], p["ny"], p["dt"], p["hx"], p["hy"], p["c1"], p["c2"], p["rho"], stype, steps)
+    got = run(libs[prec], p, g0, steps, METHODS[method], per_call=False)
+    check(prec, got, want, gd, p["nx"], p["ny"], stype, f"medium/{prec}/{stype}/{method}")
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_soa_far_end_differs_from_aos(libs, prec):
+    """le_step_soa keeps the reference SoA step's far-end rows; le_step does not."""
+    p, g0, steps = _medium(prec, ST_AOS, 64, 48, 60)
+    aos = run(libs[prec], p, g0, steps)
+    ps = dict(p, stype=ST_SOA)
+    soa = run(libs[prec], ps, aos_to_soa(g0, 64, 48), steps)
+    assert not np.allclose(aos_to_soa(aos, 64, 48), soa, rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_step_n_equals_single_steps(libs, prec):
+    """The graph-replayed multi-step call is bitwise the same as one le_step per step."""
+    p, g0, _ = _medium(prec, ST_AOS, 200, 150)
+    a = run(libs[prec], p, g0, 200, per_call=True)
+    b = run(libs[prec], p, g0, 200, per_call=False)
+    assert a.tobytes() == b.tobytes()
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_uniform_state_is_fixed_point(libs, prec):
+    c = dict(nx=257, ny=131, hx=1.0, hy=1.0, c1=2.0, c2=1.0, rho=1.0, dt=0.25, stype=ST_AOS)
+    g0 = np.tile(np.array([0.3, -0.2, 1.5, 0.25, -0.7], libs[prec].dtype), 257 * 131)
+    got = run(libs[prec], c, g0, 50, per_call=False)
+    assert got.tobytes() == g0.tobytes()
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_diagnostics_and_sim_time(libs, prec):
+    lib = libs[prec]
+    c = cases()["disks_noise_37x53"]
+    g = arrays(prec)["disks_noise_37x53__out"]
+    t = make_task(lib, c)
+    try:
+        assert lib.upload(t, g.copy()) == 0
+        rc, d = lib.diagnostics(t)
+        assert rc == 0
+        # the library computes with the material as stored in `real` (e.g. float(1.7))
+        m = [float(lib.dtype(c[k])) for k in ("hx", "hy", "c1", "c2", "rho")]
+        want = Oracle(prec).diag(g, c["nx"], c["ny"], *m, c["stype"])
+        assert abs(d["energy"] - want[0]) <= 1e-12 * abs(want[0])
+        assert np.allclose(d["sumsq"], want[1:6], rtol=1e-12, atol=0)
+        assert np.array_equal(d["maxabs"], want[6:11])
+        assert lib.step_n(t, 137) == 0
+        rc, tt, st = lib.sim_time(t)
+        acc = 0.0
+        for _ in range(137):
+            acc += float(lib.dtype(c["dt"]))
+        assert rc == 0 and st == 137 and tt == acc
+    finally:
+        lib.le_free_task(t)
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_upload_download_roundtrip(libs, prec):
+    lib = libs[prec]
+    for stype in (ST_AOS, ST_SOA):
+        c = dict(nx=131, ny=77, hx=1.0, hy=1.0, c1=2.0, c2=1.0, rho=1.0, dt=0.25, stype=stype)
+        g = np.random.default_rng(1).standard_normal(5 * 131 * 77).astype(lib.dtype)
+        t = make_task(lib, c)
+        try:
+            assert lib.upload(t, g) == 0
+            out = np.zeros_like(g)
+            assert lib.download(t, out) == 0
+            assert out.tobytes() == g.tobytes()
+        finally:
+            lib.le_free_task(t)
+
+
+def _window_parity(lib, prec, p: workloads.Problem, steps, windows):
+    """Full-size run; each window is checked against the oracle on a sub-grid that holds
+    the window plus the domain of dependence (2 nodes per sweep per step)."""
+    c = dict(nx=p.nx, ny=p.ny, hx=p.hx, hy=p.hy, c1=p.c1, c2=p.c2, rho=p.rho, dt=p.dt, stype=ST_AOS)
+    t = make_task(lib, c)
+    try:
+        for cx, cy, r, s in p.disks:
+            lib.le_set_ball(t, (cx, cy), r, s)
+        assert lib.sync_host(t) == 0
+        g0 = lib.grid_view(t).copy().reshape(p.ny, p.nx, 5)
+        assert lib.step_n(t, steps) == 0
+        assert lib.sync_host(t) == 0
+        g1 = lib.grid_view(t).reshape(p.ny, p.nx, 5)
+        m = 2 * steps
+        for (x0, y0, w, h) in windows:
+            sx0, sy0 = max(0, x0 - m), max(0, y0 - m)
+            sx1, sy1 = min(p.nx, x0 + w + m), min(p.ny, y0 + h + m)
+            sub = np.ascontiguousarray(g0[sy0:sy1, sx0:sx1]).reshape(-1)
+            for po, subp in ((prec, sub), ("d", sub.astype(np.float64))):
+                o = Oracle(po)
+                ref = subp.copy()
+                o.run(ref, sx1 - sx0, sy1 - sy0, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, ST_AOS, steps)
+                ref = ref.reshape(sy1 - sy0, sx1 - sx0, 5)[y0 - sy0:y0 - sy0 + h, x0 - sx0:x0 - sx0 + w]
+                got = g1[y0:y0 + h, x0:x0 + w]
+                a = np.ascontiguousarray(got.transpose(2, 0, 1))
+                b = np.ascontiguousarray(ref.transpose(2, 0, 1))
+                if po == prec:
+                    err = rel_l2(a, b)
+                    assert np.all(err <= TOL[prec]), ((x0, y0), err)
+                else:
+                    print(f"\nwindow {(x0, y0)} {prec}: max_abs_vs_fp64={max_abs(a, b)}")
+    finally:
+        lib.le_free_task(t)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_full_size_8192_windows(libs, prec):
+    """The 8192x8192 workload (8 seeded disks), 12 steps, windows at two disks, a corner and an edge."""
+    p = workloads.single_8192()
+    wins = []
+    for cx, cy, r, s in p.disks[:3]:  # windows across the disk rims, where the waves are
+        x0, y0 = int(cx + r) - 96, int(cy) - 96
+        wins.append((min(max(0, x0), p.nx - 192), min(max(0, y0), p.ny - 192), 192, 192))
+    wins += [(0, 0, 160, 160), (p.nx - 130, 4000, 130, 150), (3000, p.ny - 140, 170, 140)]
+    _window_parity(libs[prec], prec, p, 12, wins)
