@@ -295,18 +295,164 @@ def run_reference_arm(args):
     return 0
 
 
+def solve_plain(lib, p, per_call=True, stype=capi.ST_AOS):
+    """One solve through the single-solve API: le_init_task, le_set_ball, le_step x steps
+    (or one le2d_step_n), download of the final fields.  Returns the fields."""
+    mat = lib.le_init_material(p.c1, p.c2, p.rho)
+    t = lib.le_init_task(p.dt, (p.hx, p.hy), mat, (p.nx, p.ny), stype)
+    try:
+        for cx, cy, r, s in p.disks:
+            lib.le_set_ball(t, (cx, cy), r, s)
+        if per_call:
+            step = lib.le_step if stype == capi.ST_AOS else lib.le_step_soa
+            for _ in range(p.steps):
+                step(t)
+        else:
+            assert lib.step_n(t, p.steps) == 0
+        assert lib.sync_host(t) == 0 and lib.last_error(t) == 0
+        return lib.grid_view(t).copy()
+    finally:
+        lib.le_free_task(t)
+
+
+def run_batched(args):
+    """256 uneven FP32 solves in the persistent batched kernel vs the plain one-at-a-time loop."""
+    from oracle.oracle import fields, rel_l2
+
+    probs = workloads.batched_256()
+    lib = capi.Lib("f")
+    libd = capi.Lib("d")
+    nu = sum(p.node_updates for p in probs)
+    budget = int(1.1 * sum(2 * 5 * 4 * (((p.nx + 31) // 32) * 32) * p.ny for p in probs)) + (64 << 20)
+
+    def batch_run(scale_steps=None):
+        with capi.Batch(lib, budget) as b:
+            ids = []
+            for p in probs:
+                q = p if scale_steps is None else workloads.Problem(**{**p.__dict__, "steps": scale_steps})
+                ids.append(b.add(b.problem(q), disks=q.disks))
+            assert all(i >= 0 for i in ids)
+            t0 = time.perf_counter()
+            rc, ms = b.run(window_steps=args.window)
+            wall = time.perf_counter() - t0
+            assert rc == 0, lib.strerror(rc)
+            outs = [b.fields(i) for i in ids] if scale_steps is None else None
+            return ms, wall, outs
+
+    batch_run(scale_steps=8)  # warm-up (kernels, allocations)
+    ms, wall, outs = batch_run()
+    # the plain loop: every instance alone, one le_step call per step
+    t0 = time.perf_counter()
+    for p in probs:
+        solve_plain(lib, p, per_call=True)
+    plain_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for p in probs:
+        solve_plain(lib, p, per_call=False)
+    plain_n_s = time.perf_counter() - t0
+    # accuracy: the 8 smallest instances against the FP64 library (checked against the reference)
+    worst = np.zeros(5)
+    for k in sorted(range(len(probs)), key=lambda k: probs[k].node_updates)[:8]:
+        p = probs[k]
+        ref = solve_plain(libd, p, per_call=False)
+        err = rel_l2(fields(outs[k], p.nx, p.ny, 1), fields(ref, p.nx, p.ny, 1))
+        worst = np.maximum(worst, err)
+    line = {
+        "metric": "solves/s", "value": len(probs) / (ms * 1e-3), "unit": "solves/s", "n_gpus": 1,
+        "workload": "batched_256: 256 FP32 solves, sides log-uniform 128-2048, c1 U[1,4], c2/c1 U[0.3,0.6], "
+                    "rho U[1,3], dt=0.5h/c1, 1-4 disks, steps U[200,2000]",
+        "node_updates": nu, "batched_device_s": ms * 1e-3, "batched_wall_s": wall,
+        "batched_nu_s": nu / (ms * 1e-3), "window_steps": args.window,
+        "plain_le_step_loop_s": plain_s, "plain_le_step_solves_s": len(probs) / plain_s,
+        "plain_step_n_loop_s": plain_n_s, "plain_step_n_solves_s": len(probs) / plain_n_s,
+        "speedup_vs_plain_le_step": plain_s / (ms * 1e-3), "speedup_vs_plain_step_n": plain_n_s / (ms * 1e-3),
+        "max_rel_l2_vs_fp64_8_smallest": worst.tolist(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serving(args):
+    """Poisson request streams through the serving loop vs a one-at-a-time plain le_step server."""
+    import threading
+
+    lib = capi.Lib("f")
+    rates = [float(r) for r in args.rates.split(",")]
+    out = {"metric": "serving", "workload": "serving_stream: Poisson arrivals, sides log-uniform 64-4096, "
+                                            "materials/disks as the batched workload, steps U[100,5000], "
+                                            "half fields / half receiver lines (vx,vy at row ny/4 every 10 steps)",
+           "requests_per_rate": args.requests, "window_steps": args.window, "rates": []}
+    for rate in rates:
+        reqs = workloads.serving_stream(rate, args.requests, seed=5 + int(rate))
+        nu = sum(r.problem.node_updates for r in reqs)
+        with capi.Server(lib, args.budget << 30, window_steps=args.window) as srv:
+            tickets = [None] * len(reqs)
+
+            def submitter():
+                t0 = srv.now()
+                for k, r in enumerate(reqs):
+                    delay = t0 + r.arrival_s - srv.now()
+                    if delay > 0:
+                        time.sleep(delay)
+                    p = r.problem
+                    want = capi.LE2D_WANT_RECEIVERS if r.want == "receivers" else capi.LE2D_WANT_FIELDS
+                    prob = lib.le2d_problem(p.nx, p.ny, p.hx, p.hy, p.dt, p.c1, p.c2, p.rho, p.steps, capi.ST_AOS,
+                                            p.ny // 4 if want else -1, 10)
+                    tickets[k] = srv.submit(prob, disks=p.disks, want=want)
+
+            th = threading.Thread(target=submitter)
+            th.start()
+            th.join()
+            lat, first, last = [], None, 0.0
+            for k, t in enumerate(tickets):
+                assert t > 0 and srv.wait(t, 600.0) == 0
+                a, _, c = srv.times(t)
+                lat.append(c - a)
+                first = a if first is None else min(first, a)
+                last = max(last, c)
+                srv.release(t)
+            st = srv.stats()
+        # one-at-a-time plain le_step server on the same stream (FIFO, no overlap)
+        plat, t0, busy_until = [], time.perf_counter(), 0.0
+        for r in reqs:
+            now = time.perf_counter() - t0
+            if now < r.arrival_s:
+                time.sleep(r.arrival_s - now)
+            solve_plain(lib, r.problem, per_call=True)
+            plat.append(time.perf_counter() - t0 - r.arrival_s)
+        plain_total = time.perf_counter() - t0 - reqs[0].arrival_s
+        out["rates"].append({
+            "rate_per_s": rate, "solves_s": len(reqs) / (last - first), "node_updates_s": nu / (last - first),
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "plain_solves_s": len(reqs) / plain_total, "plain_p50_s": float(np.percentile(plat, 50)),
+            "plain_p99_s": float(np.percentile(plat, 99)), "windows": st["windows"],
+        })
+        print(json.dumps(out["rates"][-1]), file=sys.stderr, flush=True)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="single", choices=["single", "batched", "serving"])
+    ap.add_argument("--window", type=int, default=256, help="steps per persistent launch (batched/serving)")
+    ap.add_argument("--rates", default="10,50,200,2000", help="serving: request rates per second")
+    ap.add_argument("--requests", type=int, default=48, help="serving: requests per rate")
+    ap.add_argument("--budget", type=int, default=48, help="serving: HBM budget in GiB")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 leg")
     ap.add_argument("--time-steps", type=int, default=None, help="time steps per solve (default 1000)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "batched":
+        return run_batched(args)
+    if args.workload == "serving":
+        return run_serving(args)
 
     world, rank, local = dist_setup()
     backend = "nccl"

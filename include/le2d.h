@@ -67,6 +67,12 @@ int le2d_step_n_timed(le_task *task, int nsteps, float *ms);
 #define LE2D_METHOD_SPLIT 1
 int le2d_set_method(le_task *task, int method);
 
+/* Fused-kernel variant (columns per lane / register bound / unroll; -1 = default) and row
+ * segment length (0 = fill the device once) for this task's grid. */
+int le2d_set_variant(le_task *task, int variant, int seg_len);
+/* out[6] = {variant, columns per lane, segment rows, strips, warp tasks, blocks}. */
+int le2d_get_plan(const le_task *task, int *out);
+
 /* Simulated time and step count since le_init_task (FP64 accumulator). */
 int le2d_sim_time(const le_task *task, double *t, long long *steps);
 
@@ -78,6 +84,91 @@ typedef struct {
 	double maxabs[5];
 } le2d_diag_t;
 int le2d_diagnostics(le_task *task, le2d_diag_t *out);
+
+/* ---- Batched solves ------------------------------------------------------------------
+ * Many independent solves of different sizes, materials, initial conditions and step
+ * counts, advanced together by one persistent kernel over a tile work list (each tile
+ * carries its instance's material, h and dt).  The step loop runs in windows of
+ * `window_steps` steps captured in a CUDA graph. */
+typedef struct {
+	int nx, ny;            /* grid size, >= 3 each */
+	real hx, hy;           /* spacing */
+	real dt;               /* time step */
+	real c1, c2, rho;      /* material (le_init_material) */
+	int steps;             /* time steps to run */
+	int stype;             /* ST_AOS (le_step) or ST_SOA (le_step_soa semantics and layout) */
+	int receiver_row;      /* -1: none; else record vx, vy of this row every receiver_every steps */
+	int receiver_every;
+} le2d_problem;
+
+typedef struct le2d_batch le2d_batch;
+
+/* device_budget_bytes: device memory the batch may hold for states (0 = 90% of free). */
+le2d_batch *le2d_batch_create(size_t device_budget_bytes);
+void le2d_batch_destroy(le2d_batch *b);
+/* Adds an instance; its initial state is the zero grid plus `ndisks` pressure disks
+ * (disks[4k..4k+3] = cx, cy, r, s, applied in order like le_set_ball), or `init`
+ * (5*nx*ny reals in the problem's layout) when not NULL.  Returns the instance id (>= 0)
+ * or -LE2D_E* (e.g. -LE2D_EBUDGET when it does not fit the budget). */
+int le2d_batch_add(le2d_batch *b, const le2d_problem *p, const real *init, int ndisks,
+		   const real *disks);
+/* Runs every instance to its step count; *device_ms (may be NULL) = device time. */
+int le2d_batch_run(le2d_batch *b, int window_steps, float *device_ms);
+int le2d_batch_count(const le2d_batch *b);
+/* Final fields of instance `id` (5*nx*ny reals, the problem's layout). */
+int le2d_batch_fields(le2d_batch *b, int id, real *out);
+/* Receiver samples of instance `id`: out[s*2*nx + 0*nx + i] = vx, [... + 1*nx + i] = vy of
+ * sample s (after step (s+1)*receiver_every); *nsamples = steps / receiver_every. */
+int le2d_batch_receivers(le2d_batch *b, int id, real *out, int *nsamples);
+int le2d_batch_diagnostics(le2d_batch *b, int id, le2d_diag_t *out);
+/* Bounded dependency waits: the kernel gives up after this many ns (default 2e9) and
+ * le2d_batch_run returns LE2D_ETIMEOUT. */
+int le2d_batch_set_wait_limit(le2d_batch *b, unsigned long long ns);
+
+/* ---- Served solves (continuous batching) --------------------------------------------
+ * A background loop owns a device arena of `device_budget_bytes`.  Requests are queued
+ * by le2d_server_submit (thread-safe, returns at once); between windows of
+ * `window_steps` steps the loop admits queued requests while their states fit the
+ * budget (and at most `max_active` run at once), advances every admitted solve in one
+ * persistent launch, and moves finished ones to host-side results. */
+#define LE2D_WANT_FIELDS 0
+#define LE2D_WANT_RECEIVERS 1
+
+typedef struct le2d_server le2d_server;
+
+typedef struct {
+	long long submitted, admitted, completed, failed;
+	long long node_updates;   /* node-updates done by the device */
+	long long windows;        /* persistent launches */
+	double device_busy_s;     /* host time spent in launches */
+	size_t arena_used, arena_capacity;
+	int active, queued;
+} le2d_server_stats_t;
+
+le2d_server *le2d_server_create(size_t device_budget_bytes, int window_steps, int max_active);
+/* Stops the loop; unfinished requests are dropped. */
+void le2d_server_destroy(le2d_server *s);
+/* Queues a solve (init/disks as le2d_batch_add; `init` is copied).  `want` =
+ * LE2D_WANT_FIELDS or LE2D_WANT_RECEIVERS (needs p->receiver_row >= 0).  Returns a ticket
+ * (>= 1) or -LE2D_E* (EINVAL: bad request; EBUDGET: larger than the whole budget). */
+long long le2d_server_submit(le2d_server *s, const le2d_problem *p, const real *init, int ndisks,
+			     const real *disks, int want);
+/* 1 = finished, 0 = pending, -LE2D_E* = failed or unknown ticket. */
+int le2d_server_poll(le2d_server *s, long long ticket);
+/* Waits up to timeout_s (< 0: no limit): LE2D_OK, LE2D_ETIMEOUT, or the request's error. */
+int le2d_server_wait(le2d_server *s, long long ticket, double timeout_s);
+/* Copies a finished result: fields (5*nx*ny reals, problem layout) or receiver samples
+ * ([nsamples][2][nx]); out_elems = capacity of `out`; *nsamples set for receivers. */
+int le2d_server_result(le2d_server *s, long long ticket, real *out, size_t out_elems,
+		       int *nsamples);
+/* Host monotonic times (s) of submission, admission to the device and completion. */
+int le2d_server_times(le2d_server *s, long long ticket, double *t_submit, double *t_admit,
+		      double *t_done);
+/* Forgets a finished ticket and its result. */
+int le2d_server_release(le2d_server *s, long long ticket);
+int le2d_server_stats(le2d_server *s, le2d_server_stats_t *out);
+/* Host monotonic clock used by le2d_server_times (s). */
+double le2d_now(void);
 
 /* Layout of the device state (SoA, 5 planes of n.y rows with a padded row pitch). */
 int le2d_device_layout(const le_task *task, long long *pitch_elems, long long *plane_elems);

@@ -38,9 +38,26 @@ EXPORTS = [
     "le_init_material", "le_init_task", "le_free_task", "le_set_ball", "le_save_task", "le_step",
     "le_step_soa", "le2d_strerror", "le2d_set_device", "le2d_last_error", "le2d_clear_error", "le2d_sync_host",
     "le2d_sync_device", "le2d_wait", "le2d_upload", "le2d_download", "le2d_step_n",
-    "le2d_step_n_timed", "le2d_set_method", "le2d_sim_time", "le2d_diagnostics",
+    "le2d_step_n_timed", "le2d_set_method", "le2d_set_variant", "le2d_get_plan", "le2d_sim_time",
+    "le2d_diagnostics",
     "le2d_device_layout", "le2d_task_device_bytes", "le2d_host_alloc", "le2d_host_free",
+    "le2d_batch_create", "le2d_batch_destroy", "le2d_batch_add", "le2d_batch_run", "le2d_batch_count",
+    "le2d_batch_fields", "le2d_batch_receivers", "le2d_batch_diagnostics", "le2d_batch_set_wait_limit",
+    "le2d_server_create", "le2d_server_destroy", "le2d_server_submit", "le2d_server_poll",
+    "le2d_server_wait", "le2d_server_result", "le2d_server_times", "le2d_server_release",
+    "le2d_server_stats", "le2d_now",
 ]
+
+LE2D_WANT_FIELDS = 0
+LE2D_WANT_RECEIVERS = 1
+
+
+class le2d_server_stats_t(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("admitted", ctypes.c_longlong),
+                ("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+                ("node_updates", ctypes.c_longlong), ("windows", ctypes.c_longlong),
+                ("device_busy_s", ctypes.c_double), ("arena_used", ctypes.c_size_t),
+                ("arena_capacity", ctypes.c_size_t), ("active", ctypes.c_int), ("queued", ctypes.c_int)]
 
 
 class LibraryMissing(RuntimeError):
@@ -71,7 +88,12 @@ def _types(prec: str):
         _fields_ = [("energy", ctypes.c_double), ("sumsq", ctypes.c_double * 5),
                     ("maxabs", ctypes.c_double * 5)]
 
-    return real, le_vec2, le_point2, le_material, le_task, le2d_diag_t
+    class le2d_problem(ctypes.Structure):
+        _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("hx", real), ("hy", real), ("dt", real),
+                    ("c1", real), ("c2", real), ("rho", real), ("steps", ctypes.c_int), ("stype", ctypes.c_int),
+                    ("receiver_row", ctypes.c_int), ("receiver_every", ctypes.c_int)]
+
+    return real, le_vec2, le_point2, le_material, le_task, le2d_diag_t, le2d_problem
 
 
 class Lib:
@@ -85,7 +107,7 @@ class Lib:
         self.dtype = np.float32 if prec == "f" else np.float64
         self.lib = ctypes.CDLL(path)
         (self.real, self.le_vec2, self.le_point2, self.le_material, self.le_task,
-         self.le2d_diag_t) = _types(prec)
+         self.le2d_diag_t, self.le2d_problem) = _types(prec)
         L, R = self.lib, self.real
         P = ctypes.POINTER
         L.le_init_material.argtypes = [R, R, R, P(self.le_material)]
@@ -113,6 +135,8 @@ class Lib:
         L.le2d_step_n.argtypes = [P(self.le_task), ctypes.c_int]
         L.le2d_step_n_timed.argtypes = [P(self.le_task), ctypes.c_int, P(ctypes.c_float)]
         L.le2d_set_method.argtypes = [P(self.le_task), ctypes.c_int]
+        L.le2d_set_variant.argtypes = [P(self.le_task), ctypes.c_int, ctypes.c_int]
+        L.le2d_get_plan.argtypes = [P(self.le_task), P(ctypes.c_int)]
         L.le2d_sim_time.argtypes = [P(self.le_task), P(ctypes.c_double), P(ctypes.c_longlong)]
         L.le2d_diagnostics.argtypes = [P(self.le_task), P(self.le2d_diag_t)]
         L.le2d_device_layout.argtypes = [P(self.le_task), P(ctypes.c_longlong), P(ctypes.c_longlong)]
@@ -122,6 +146,34 @@ class Lib:
         L.le2d_host_alloc.restype = ctypes.c_void_p
         L.le2d_host_free.argtypes = [ctypes.c_void_p]
         L.le2d_host_free.restype = None
+        L.le2d_batch_create.argtypes = [ctypes.c_size_t]
+        L.le2d_batch_create.restype = ctypes.c_void_p
+        L.le2d_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.le2d_batch_destroy.restype = None
+        L.le2d_batch_add.argtypes = [ctypes.c_void_p, P(self.le2d_problem), ctypes.c_void_p, ctypes.c_int,
+                                     ctypes.c_void_p]
+        L.le2d_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_int, P(ctypes.c_float)]
+        L.le2d_batch_count.argtypes = [ctypes.c_void_p]
+        L.le2d_batch_fields.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.le2d_batch_receivers.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, P(ctypes.c_int)]
+        L.le2d_batch_diagnostics.argtypes = [ctypes.c_void_p, ctypes.c_int, P(self.le2d_diag_t)]
+        L.le2d_batch_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong]
+        L.le2d_server_create.argtypes = [ctypes.c_size_t, ctypes.c_int, ctypes.c_int]
+        L.le2d_server_create.restype = ctypes.c_void_p
+        L.le2d_server_destroy.argtypes = [ctypes.c_void_p]
+        L.le2d_server_destroy.restype = None
+        L.le2d_server_submit.argtypes = [ctypes.c_void_p, P(self.le2d_problem), ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_int]
+        L.le2d_server_submit.restype = ctypes.c_longlong
+        L.le2d_server_poll.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
+        L.le2d_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double]
+        L.le2d_server_result.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_size_t,
+                                         P(ctypes.c_int)]
+        L.le2d_server_times.argtypes = [ctypes.c_void_p, ctypes.c_longlong, P(ctypes.c_double),
+                                        P(ctypes.c_double), P(ctypes.c_double)]
+        L.le2d_server_release.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
+        L.le2d_server_stats.argtypes = [ctypes.c_void_p, P(le2d_server_stats_t)]
+        L.le2d_now.restype = ctypes.c_double
 
     # --- the reference task API, same names ---
     def le_init_material(self, c1, c2, rho):
@@ -190,6 +242,16 @@ class Lib:
     def set_method(self, t, method: int) -> int:
         return self.lib.le2d_set_method(ctypes.byref(t), method)
 
+    def set_variant(self, t, variant: int, seg_len: int = 0) -> int:
+        return self.lib.le2d_set_variant(ctypes.byref(t), variant, seg_len)
+
+    def get_plan(self, t) -> dict:
+        out = (ctypes.c_int * 6)()
+        rc = self.lib.le2d_get_plan(ctypes.byref(t), out)
+        if rc:
+            raise RuntimeError(self.strerror(rc))
+        return dict(zip(("variant", "lanes", "seg_len", "nstrips", "ntasks", "blocks"), list(out)))
+
     def sim_time(self, t):
         tt, st = ctypes.c_double(0.0), ctypes.c_longlong(0)
         rc = self.lib.le2d_sim_time(ctypes.byref(t), ctypes.byref(tt), ctypes.byref(st))
@@ -222,6 +284,150 @@ class Lib:
         """The host grid (task->grid) as a numpy array (no copy)."""
         n = 5 * t.n.x * t.n.y
         return np.ctypeslib.as_array(t.grid, shape=(n,))
+
+
+class Batch:
+    """le2d_batch_*: many independent solves advanced by one persistent kernel."""
+
+    def __init__(self, lib: Lib, budget_bytes: int = 0):
+        self.lib = lib
+        self.h = lib.lib.le2d_batch_create(budget_bytes)
+        if not self.h:
+            raise RuntimeError("le2d_batch_create failed")
+        self.problems = []
+
+    def close(self):
+        if self.h:
+            self.lib.lib.le2d_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def problem(self, p, stype=ST_AOS, receiver_row=-1, receiver_every=10):
+        """A le2d_problem from a workloads.Problem."""
+        return self.lib.le2d_problem(p.nx, p.ny, p.hx, p.hy, p.dt, p.c1, p.c2, p.rho, p.steps, stype,
+                                     receiver_row, receiver_every)
+
+    def add(self, prob, init: np.ndarray | None = None, disks=()) -> int:
+        d = np.ascontiguousarray(np.asarray(disks, dtype=self.lib.dtype).reshape(-1))
+        ip = None
+        if init is not None:
+            init = np.ascontiguousarray(init, dtype=self.lib.dtype)
+            ip = init.ctypes.data
+        rid = self.lib.lib.le2d_batch_add(self.h, ctypes.byref(prob), ip, len(d) // 4,
+                                          d.ctypes.data if len(d) else None)
+        if rid >= 0:
+            self.problems.append(prob)
+        return rid
+
+    def run(self, window_steps: int = 256):
+        ms = ctypes.c_float(0.0)
+        rc = self.lib.lib.le2d_batch_run(self.h, window_steps, ctypes.byref(ms))
+        return rc, ms.value
+
+    def fields(self, rid: int) -> np.ndarray:
+        p = self.problems[rid]
+        out = np.zeros(5 * p.nx * p.ny, self.lib.dtype)
+        rc = self.lib.lib.le2d_batch_fields(self.h, rid, out.ctypes.data)
+        if rc:
+            raise RuntimeError(self.lib.strerror(rc))
+        return out
+
+    def receivers(self, rid: int) -> np.ndarray:
+        p = self.problems[rid]
+        n = ctypes.c_int(0)
+        rc = self.lib.lib.le2d_batch_receivers(self.h, rid, None, ctypes.byref(n))
+        out = np.zeros((n.value, 2, p.nx), self.lib.dtype)
+        rc = self.lib.lib.le2d_batch_receivers(self.h, rid, out.ctypes.data, ctypes.byref(n))
+        if rc:
+            raise RuntimeError(self.lib.strerror(rc))
+        return out
+
+    def diagnostics(self, rid: int):
+        d = self.lib.le2d_diag_t()
+        rc = self.lib.lib.le2d_batch_diagnostics(self.h, rid, ctypes.byref(d))
+        return rc, {"energy": d.energy, "sumsq": list(d.sumsq), "maxabs": list(d.maxabs)}
+
+    def set_wait_limit(self, ns: int) -> int:
+        return self.lib.lib.le2d_batch_set_wait_limit(self.h, ns)
+
+
+class Server:
+    """le2d_server_*: continuous-batching request loop (a background thread in the library)."""
+
+    def __init__(self, lib: Lib, budget_bytes: int = 0, window_steps: int = 100, max_active: int = 1024):
+        self.lib = lib
+        self.h = lib.lib.le2d_server_create(budget_bytes, window_steps, max_active)
+        if not self.h:
+            raise RuntimeError("le2d_server_create failed")
+        self.meta = {}
+
+    def close(self):
+        if self.h:
+            self.lib.lib.le2d_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, prob, init=None, disks=(), want=LE2D_WANT_FIELDS) -> int:
+        d = np.ascontiguousarray(np.asarray(disks, dtype=self.lib.dtype).reshape(-1))
+        ip = None
+        if init is not None:
+            init = np.ascontiguousarray(init, dtype=self.lib.dtype)
+            ip = init.ctypes.data
+        t = self.lib.lib.le2d_server_submit(self.h, ctypes.byref(prob), ip, len(d) // 4,
+                                            d.ctypes.data if len(d) else None, want)
+        if t > 0:
+            self.meta[t] = (prob.nx, prob.ny, want)
+        return t
+
+    def poll(self, ticket) -> int:
+        return self.lib.lib.le2d_server_poll(self.h, ticket)
+
+    def wait(self, ticket, timeout_s: float = -1.0) -> int:
+        return self.lib.lib.le2d_server_wait(self.h, ticket, timeout_s)
+
+    def result(self, ticket) -> np.ndarray:
+        nx, ny, want = self.meta[ticket]
+        n = ctypes.c_int(0)
+        if want == LE2D_WANT_FIELDS:
+            out = np.zeros(5 * nx * ny, self.lib.dtype)
+        else:
+            rc = self.lib.lib.le2d_server_result(self.h, ticket, None, 0, ctypes.byref(n))
+            if rc:
+                raise RuntimeError(self.lib.strerror(rc))
+            out = np.zeros((n.value, 2, nx), self.lib.dtype)
+        rc = self.lib.lib.le2d_server_result(self.h, ticket, out.ctypes.data, out.size, ctypes.byref(n))
+        if rc:
+            raise RuntimeError(self.lib.strerror(rc))
+        return out
+
+    def times(self, ticket):
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        rc = self.lib.lib.le2d_server_times(self.h, ticket, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        if rc:
+            raise RuntimeError(self.lib.strerror(rc))
+        return a.value, b.value, c.value
+
+    def release(self, ticket) -> int:
+        self.meta.pop(ticket, None)
+        return self.lib.lib.le2d_server_release(self.h, ticket)
+
+    def stats(self) -> dict:
+        s = le2d_server_stats_t()
+        self.lib.lib.le2d_server_stats(self.h, ctypes.byref(s))
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def now(self) -> float:
+        return self.lib.lib.le2d_now()
 
 
 def material_array(lib: Lib, m) -> np.ndarray:

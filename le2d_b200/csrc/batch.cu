@@ -1,0 +1,167 @@
+// Batched persistent step kernel: many independent solves of different sizes,
+// materials and step counts advance together in one launch.
+//
+// Work list.  Every instance is cut into tiles (strip x row segment, one warp each,
+// marched by the same body as the single-solve kernel, march.cuh).  A launch covers
+// a window of steps; the work items are (window step r, tile) in step-major order,
+// where the tiles of step r are a prefix of the tile list (instances are ordered by
+// their step count in the window, longest first).  Warps claim items with one atomic
+// counter and loop until the list is empty.
+//
+// Dependencies instead of grid barriers.  Tile t at step r reads the state its 3x3
+// neighbourhood of tiles wrote at step r-1 (2 halo rows, 2 halo columns), and writes
+// the buffer those tiles read at step r-1.  So before item (r, t) the warp waits until
+// done[n] >= r for every neighbour n (and t itself); after the tile it publishes
+// done[t] = r + 1 with release semantics.  Items are claimed in order and a claimed
+// item only waits on items of smaller index, all held by running warps, so the
+// smallest unfinished item can always proceed.  Every wait is bounded: after
+// `wait_ns` of global time (or once another warp has given up) the warp sets
+// ctl->status and leaves; the host reads the status (LE2D_ETIMEOUT), the context stays
+// usable.  State loads use ld.global.cg: other warps of this launch write them.
+#include "march.cuh"
+
+namespace le2d {
+
+namespace {
+
+constexpr int kWarps = 4;
+constexpr int kLanes = 4;  // columns per lane (FP32)
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits until every tile of the 3x3 neighbourhood of (seg, strip) has done[] >= r.
+// Lanes 0..8 each watch one neighbour.  Returns false if the wait gave up.
+__device__ __forceinline__ bool wait_neighbours(const int* done, int tile_base, int nstrips,
+                                                int nsegs, int seg, int strip, int r,
+                                                BatchCtl* ctl, unsigned long long wait_ns) {
+  const int lane = threadIdx.x & 31;
+  const int ds = lane / 3 - 1, dk = lane % 3 - 1;
+  const int s2 = seg + ds, k2 = strip + dk;
+  const bool watch = lane < 9 && s2 >= 0 && s2 < nsegs && k2 >= 0 && k2 < nstrips;
+  const int* p = done + tile_base + (watch ? s2 * nstrips + k2 : 0);
+  const unsigned long long t0 = global_ns();
+  unsigned ns = 32;
+  while (true) {
+    const bool ready = !watch || ld_acquire(p) >= r;
+    if (__all_sync(0xffffffffu, ready)) return true;
+    int bail = 0;
+    if (lane == 0) {
+      bail = *reinterpret_cast<volatile int*>(&ctl->status) != 0;
+      if (!bail && global_ns() - t0 > wait_ns) {
+        atomicExch(&ctl->status, 1);
+        bail = 1;
+      }
+    }
+    if (__shfl_sync(0xffffffffu, bail, 0)) return false;
+    __nanosleep(ns);
+    if (ns < 1024) ns *= 2;
+  }
+}
+
+template <typename T, int V, int MINB>
+__global__ void __launch_bounds__(kWarps * 32, MINB)
+    batch_kernel(const BatchInst<T>* __restrict__ insts, const BatchTile* __restrict__ tiles,
+                 const long long* __restrict__ step_items, int nsteps, int* done, BatchCtl* ctl,
+                 unsigned long long wait_ns, int stall_plus1) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  T* ring = reinterpret_cast<T*>(smem_raw) + (threadIdx.x >> 5) * (3 * NF * 32 * V);
+  const long long total = step_items[nsteps];
+  int r = 0;
+  while (true) {
+    unsigned long long q = 0;
+    if (lane == 0) q = atomicAdd(&ctl->next, 1ULL);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if ((long long)q >= total) break;
+    while ((long long)q >= step_items[r + 1]) ++r;
+    const BatchTile bt = tiles[q - step_items[r]];
+    const BatchInst<T>& I = insts[bt.inst];
+    if (r > 0 &&
+        !wait_neighbours(done, I.tile_base, I.nstrips, I.nsegs, bt.seg, bt.strip, r, ctl, wait_ns))
+      break;
+    const int par = (I.parity + r) & 1;
+    const march::GridRef<T> g{I.buf[par], I.buf[par ^ 1], I.nx, I.ny, I.pitch, I.plane, I.far_rot};
+    const int y0 = bt.seg * I.seg_len;
+    const int y1 = min(y0 + I.seg_len, I.ny);
+    march::RowTap<T> tap{nullptr, -1};
+    const long long step_after = I.abs_step0 + r + 1;  // absolute step count after this step
+    if (I.trace != nullptr && step_after % I.trace_every == 0)
+      tap = march::RowTap<T>{I.trace + (step_after / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
+    march::march_tile<T, V, 1, true, true>(g, I.c, bt.strip, y0, y1, ring, tap);
+    __syncwarp();
+    const int tile_id = I.tile_base + bt.seg * I.nstrips + bt.strip;
+    if (lane == 0 && !(r == 0 && tile_id == stall_plus1 - 1)) {
+      __threadfence();
+      st_release(done + tile_id, r + 1);
+    }
+  }
+}
+
+template <typename T>
+struct BatchKernelOf;
+template <>
+struct BatchKernelOf<float> {
+  static constexpr int V = 4, MINB = 3;
+};
+template <>
+struct BatchKernelOf<double> {
+  static constexpr int V = 2, MINB = 2;
+};
+
+}  // namespace
+
+template <typename T>
+int batch_lanes() { return BatchKernelOf<T>::V; }
+
+template <typename T>
+size_t batch_smem() { return (size_t)kWarps * 3 * NF * 32 * BatchKernelOf<T>::V * sizeof(T); }
+
+template <typename T>
+int batch_resident_blocks(int device) {
+  using K = BatchKernelOf<T>;
+  int sms = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<T, K::V, K::MINB>,
+                                                    kWarps * 32, batch_smem<T>()) != cudaSuccess)
+    return 0;
+  return sms * per_sm;
+}
+
+template <typename T>
+cudaError_t launch_batch(const BatchInst<T>* insts, const BatchTile* tiles,
+                         const long long* step_items, int nsteps, long long total_items, int* done,
+                         BatchCtl* ctl, unsigned long long wait_ns, int stall_plus1,
+                         int resident_blocks, cudaStream_t s) {
+  using K = BatchKernelOf<T>;
+  long long blocks = (total_items + kWarps - 1) / kWarps;
+  if (blocks > resident_blocks) blocks = resident_blocks;
+  if (blocks < 1) blocks = 1;
+  batch_kernel<T, K::V, K::MINB><<<(int)blocks, kWarps * 32, batch_smem<T>(), s>>>(
+      insts, tiles, step_items, nsteps, done, ctl, wait_ns, stall_plus1);
+  return cudaGetLastError();
+}
+
+#define LE2D_INST(T)                                                                            \
+  template int batch_lanes<T>();                                                                \
+  template size_t batch_smem<T>();                                                              \
+  template int batch_resident_blocks<T>(int);                                                   \
+  template cudaError_t launch_batch<T>(const BatchInst<T>*, const BatchTile*, const long long*, \
+                                       int, long long, int*, BatchCtl*, unsigned long long, int, \
+                                       int, cudaStream_t);
+LE2D_INST(float)
+LE2D_INST(double)
+#undef LE2D_INST
+
+}  // namespace le2d

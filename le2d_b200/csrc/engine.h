@@ -1,0 +1,119 @@
+// Host side of batched and served solves: a device arena for instance states, the
+// per-window work lists of the persistent kernel (batch.cu), and result read-back.
+// Used by le2d_batch_* (all instances known up front, windows captured in one CUDA
+// graph) and by the serving loop (instances join and leave between windows).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <map>
+#include <vector>
+
+#include "le2d.h"
+#include "le2d_kernels.h"
+
+namespace le2d {
+
+// First-fit allocator over one cudaMalloc'd block; offsets are 256-byte aligned.
+class Arena {
+ public:
+  explicit Arena(size_t capacity);
+  ~Arena();
+  bool ok() const { return base_ != nullptr; }
+  // Returns an offset or SIZE_MAX when `bytes` does not fit.
+  size_t alloc(size_t bytes);
+  void free(size_t off);
+  size_t capacity() const { return cap_; }
+  size_t used() const { return used_; }
+  char* base() const { return base_; }
+
+ private:
+  char* base_ = nullptr;
+  size_t cap_ = 0, used_ = 0;
+  std::map<size_t, size_t> free_;  // offset -> size
+  std::map<size_t, size_t> live_;  // offset -> size
+};
+
+template <typename T>
+class Engine {
+ public:
+  struct Inst {
+    le2d_problem p;
+    long long pitch = 0, plane = 0;
+    size_t state_off = SIZE_MAX, trace_off = SIZE_MAX;
+    T* buf[2] = {nullptr, nullptr};
+    T* trace = nullptr;
+    int nsamples = 0;
+    long long done_steps = 0;
+    StepConsts<T> c;
+    int nstrips = 0, nsegs = 0, seg_len = 0;
+    bool live = false;
+  };
+
+  explicit Engine(size_t budget_bytes);
+  ~Engine();
+  bool ok() const { return arena_ && arena_->ok() && stream_ != nullptr; }
+  cudaStream_t stream() const { return stream_; }
+
+  // Device bytes an instance of this problem holds (states + receiver samples).
+  static size_t footprint(const le2d_problem& p);
+  // Validates, allocates and initialises an instance; returns its id or -LE2D_E*.
+  int add(const le2d_problem& p, const T* init, int ndisks, const T* disks);
+  // Advances every live instance with steps left by min(left, window) steps in one
+  // persistent launch (not captured); returns LE2D_OK / LE2D_ETIMEOUT / LE2D_ECUDA.
+  int run_window(int window);
+  // Runs every live instance to completion: all windows captured in one CUDA graph.
+  int run_all(int window, float* ms);
+  int fields(int id, T* out);
+  int receivers(int id, T* out, int* nsamples);
+  int diagnostics(int id, le2d_diag_t* out);
+  // Releases the instance's device memory (its results must have been read).
+  void release(int id);
+  bool finished(int id) const;
+  int count() const { return (int)insts_.size(); }
+  const Inst& inst(int id) const { return insts_[id]; }
+  void set_wait_ns(unsigned long long ns) { wait_ns_ = ns; }
+  int set_seg_len(int rows);
+  size_t arena_used() const { return arena_ ? arena_->used() : 0; }
+  size_t arena_capacity() const { return arena_ ? arena_->capacity() : 0; }
+  long long node_updates() const { return node_updates_; }
+
+ private:
+  struct Window {
+    std::vector<BatchInst<T>> insts;
+    std::vector<BatchTile> tiles;
+    std::vector<long long> step_items;  // size steps+1
+    std::vector<int> inst_ids;
+    std::vector<int> inst_steps;
+    int steps = 0;
+  };
+  Window plan_window(int window, const std::vector<long long>& done_steps) const;
+  int ensure_scratch(size_t insts, size_t tiles, size_t items, size_t done, size_t ctls);
+  int launch_window(const Window& w, size_t inst_off, size_t tile_off, size_t item_off,
+                    size_t done_off, size_t ctl_off);
+
+  Arena* arena_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+  std::vector<Inst> insts_;
+  unsigned long long wait_ns_ = 2000000000ULL;
+  int stall_tile_ = -1;  // test hook from LE2D_TEST_STALL_TILE (see launch_batch)
+  int seg_len_ = 64;
+  int resident_blocks_ = 0;
+  long long node_updates_ = 0;
+  // device scratch of the persistent launches (work lists, counters)
+  BatchInst<T>* d_insts_ = nullptr;
+  BatchTile* d_tiles_ = nullptr;
+  long long* d_items_ = nullptr;
+  int* d_done_ = nullptr;
+  BatchCtl* d_ctl_ = nullptr;
+  size_t cap_insts_ = 0, cap_tiles_ = 0, cap_items_ = 0, cap_done_ = 0, cap_ctl_ = 0;
+  double* d_diag_ = nullptr;
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
+};
+
+// Constants of one problem's step (same derivation as the single-solve path).
+template <typename T>
+StepConsts<T> problem_consts(const le2d_problem& p);
+
+}  // namespace le2d

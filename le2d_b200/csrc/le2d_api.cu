@@ -22,6 +22,7 @@
 #include <mutex>
 #include <unordered_map>
 
+#include "consts.h"
 #include "le2d.h"
 #include "le2d_kernels.h"
 
@@ -89,40 +90,39 @@ DevTask* lookup(const le_task* task) {
   return it == g_tasks.end() ? nullptr : it->second;
 }
 
-long long row_pitch(int nx) {
-  const int align = 128 / (int)sizeof(T);  // 128-byte rows
-  return ((long long)nx + align - 1) / align * align;
+long long row_pitch(int nx) { return le2d::row_pitch_elems(nx); }
+
+// Fused-kernel variant used for new tasks: LE2D_FUSED_VARIANT if set, else 0.
+int default_variant() {
+  static int v = -2;
+  if (v == -2) {
+    const char* e = getenv("LE2D_FUSED_VARIANT");
+    v = e ? atoi(e) : 0;
+    if (v < 0 || v >= le2d::fused_variant_count<T>()) v = 0;
+  }
+  return v;
 }
 
-// Sweep constants of an axis with spacing h.  k1, k2 as the reference computes them,
-// in real (simple/le_core.c:468-469, :511-512); derived factors rounded once from double.
-Sweep<T> make_sweep(const le_task* t, T h) {
-  const T k1 = t->dt * t->mat.c1 / h;
-  const T k2 = t->dt * t->mat.c2 / h;
-  Sweep<T> s;
-  s.irhoc1 = t->mat.irhoc1;
-  s.irhoc2 = t->mat.irhoc2;
-  s.kc1 = (T)((1.0 - (double)k1) / 2.0);
-  s.kc2 = (T)((1.0 - (double)k2) / 2.0);
-  s.hk1 = (T)(0.5 * (double)k1);
-  s.hk2 = (T)(0.5 * (double)k2);
-  s.hk1rc1 = (T)(0.5 * (double)k1 * (double)t->mat.rhoc1);
-  s.hk1rc3 = (T)(0.5 * (double)k1 * (double)t->mat.rhoc3);
-  s.hk2rc2 = (T)(0.5 * (double)k2 * (double)t->mat.rhoc2);
-  s.k1 = k1;
-  s.k2 = k2;
-  s.rhoc1 = t->mat.rhoc1;
-  s.rhoc2 = t->mat.rhoc2;
-  s.rhoc3 = t->mat.rhoc3;
-  return s;
+// Work decomposition of the fused kernel for this task; seg_len 0 = fill the device once.
+void replan(DevTask* d, int variant, int seg_len) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int resident = le2d::fused_resident_warps<T>(dev, variant);
+  le2d::FusedPlan p = le2d::plan_fused<T>(d->nx, d->ny, variant, resident, kMinSeg);
+  if (seg_len > 0) {  // explicit segment length (tuning)
+    const int wpb = p.threads / 32;
+    p.seg_len = seg_len < d->ny ? seg_len : d->ny;
+    p.nsegs = (d->ny + p.seg_len - 1) / p.seg_len;
+    p.ntasks = p.nstrips * p.nsegs;
+    p.blocks = (p.ntasks + wpb - 1) / wpb;
+  }
+  d->plan = p;
+  if (d->graph) cudaGraphExecDestroy(d->graph);
+  d->graph = nullptr;
 }
 
-StepConsts<T> make_consts(const le_task* t) {
-  StepConsts<T> c;
-  c.x = make_sweep(t, t->h.x);
-  c.y = make_sweep(t, t->h.y);
-  return c;
-}
+// Step constants from the task as it is now (the caller may change dt between steps).
+StepConsts<T> make_consts(const le_task* t) { return le2d::make_consts(t->dt, t->h, t->mat); }
 
 bool same_consts(const StepConsts<T>& a, const StepConsts<T>& b) {
   return memcmp(&a, &b, sizeof(a)) == 0;
@@ -390,9 +390,7 @@ void le_init_task(le_task* task, const real dt, const le_vec2 h, const le_materi
         record(d, LE2D_ECUDA, "le_init_task: device setup", e);
         d->has_device = false;
       }
-      int dev = 0;
-      cudaGetDevice(&dev);
-      d->plan = le2d::plan_fused<T>(n.x, n.y, le2d::fused_resident_warps<T>(dev), kMinSeg);
+      replan(d, default_variant(), 0);
     }
   } else {
     record(d, LE2D_ENODEV, "le_init_task");
@@ -573,6 +571,28 @@ int le2d_set_method(le_task* task, int method) {
   if (!d) return LE2D_ENOTASK;
   if (method != LE2D_METHOD_FUSED && method != LE2D_METHOD_SPLIT) return LE2D_EINVAL;
   d->method = method;
+  return LE2D_OK;
+}
+
+int le2d_set_variant(le_task* task, int variant, int seg_len) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  if (variant < -1 || variant >= le2d::fused_variant_count<T>() || seg_len < 0) return LE2D_EINVAL;
+  if (!d->has_device) return LE2D_ENODEV;
+  replan(d, variant < 0 ? default_variant() : variant, seg_len);
+  return LE2D_OK;
+}
+
+int le2d_get_plan(const le_task* task, int* out) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  if (!out) return LE2D_EINVAL;
+  out[0] = d->plan.variant;
+  out[1] = d->plan.lanes;
+  out[2] = d->plan.seg_len;
+  out[3] = d->plan.nstrips;
+  out[4] = d->plan.ntasks;
+  out[5] = d->plan.blocks;
   return LE2D_OK;
 }
 

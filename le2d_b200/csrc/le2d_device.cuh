@@ -68,10 +68,15 @@ __device__ __forceinline__ float max3(float a, float b, float c) {
 __device__ __forceinline__ double max3(double a, double b, double c) { return fmax(a, fmax(b, c)); }
 
 // kc * superbee(r), superbee(r) = max(0, min(1, 2r), min(2, r))  (simple/le_core.c:38).
-// fmin returns the non-NaN operand, so superbee(NaN) = max(0, 1, 2) = 2 as in le_min/le_max.
-template <typename T>
-__device__ __forceinline__ T psi(T r, T kc) {
-  return kc * max3(T(0), fmin(T(1), r + r), fmin(T(2), r));
+// FP64: as written; fmin returns the non-NaN operand, so superbee(NaN) = max(0, 1, 2) = 2
+// as the reference's le_min/le_max give.  FP32: max(sat(2r), min(2, r)), the same
+// function with one min/max less -- sat clamps 2r to [0, 1] (so r <= 0 gives 0 from both
+// terms) and flushes NaN to 0, while min(2, NaN) = 2, keeping superbee(NaN) = 2.
+__device__ __forceinline__ float psi(float r, float kc) {
+  return kc * fmaxf(__saturatef(r + r), fminf(2.0f, r));
+}
+__device__ __forceinline__ double psi(double r, double kc) {
+  return kc * max3(0.0, fmin(1.0, r + r), fmin(2.0, r));
 }
 
 // Limited flux of a right-moving invariant through the face right of node i.

@@ -11,22 +11,30 @@ namespace le2d {
 
 // Work decomposition of the fused step: the grid is cut into vertical strips of
 // strip_out columns (one warp each) and each strip into segments of seg_len rows.
+// A strip is 32 lanes x `lanes` columns.  The x-stencil reaches two nodes each way, so
+// the outermost halo_lanes() lanes on each side only supply neighbours.
+__host__ __device__ constexpr int halo_lanes(int lanes) { return lanes >= 2 ? 1 : 2; }
+__host__ __device__ constexpr int strip_cols(int lanes) { return (32 - 2 * halo_lanes(lanes)) * lanes; }
+
 struct FusedPlan {
+  int variant = 0, lanes = 0;
   int nstrips = 0, seg_len = 0, nsegs = 0, ntasks = 0;
   int blocks = 0, threads = 0;
   size_t smem = 0;
 };
 
-// Outputs per warp strip: 30 of the 32 lanes, V = 16 / sizeof(T) columns each.
+// Compiled kernel variants (columns per lane, register bound, loop unroll).
 template <typename T>
-constexpr int strip_out() { return 30 * (16 / (int)sizeof(T)); }
+int fused_variant_count();
+template <typename T>
+int fused_variant_lanes(int variant);
 
 template <typename T>
-FusedPlan plan_fused(int nx, int ny, int resident_warps, int min_seg);
+FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_seg);
 
-// Warps of the fused kernel that fit on the device at once.
+// Warps of the fused kernel variant that fit on the device at once.
 template <typename T>
-int fused_resident_warps(int device);
+int fused_resident_warps(int device, int variant);
 
 // One fused time step src -> dst.  far_rot selects the le_step_soa far-end rows.
 template <typename T>
@@ -53,6 +61,51 @@ cudaError_t launch_unpack(const T* soa, T* raw, int nx, int ny, long long pitch,
 template <typename T>
 cudaError_t launch_set_ball(T* soa, int nx, int ny, long long pitch, long long plane, T hx, T hy,
                             T cx, T cy, T r, T s_val, cudaStream_t s);
+
+// ---- batched persistent kernel (batch.cu) ----
+
+// One instance within one launch window (device-resident array).
+template <typename T>
+struct BatchInst {
+  T* buf[2];             // the two state buffers (pitched SoA)
+  int nx, ny;
+  long long pitch, plane;
+  StepConsts<T> c;
+  int far_rot;           // le_step_soa far-end rows
+  int nstrips, nsegs, seg_len;
+  int tile_base;         // index of the instance's first tile in the tile list and done[]
+  int parity;            // buffer holding the state at window step 0
+  int steps;             // steps of this instance in the window
+  long long abs_step0;   // steps the instance had done before the window
+  T* trace;              // receiver samples [sample][2][pitch], or null
+  int trace_row;         // receiver row
+  int trace_every;       // steps between samples
+};
+
+struct BatchTile {
+  int inst, strip, seg, pad;
+};
+
+struct BatchCtl {
+  unsigned long long next;  // next work item
+  int status;               // 0 = ok, 1 = a dependency wait gave up
+  int pad;
+};
+
+template <typename T>
+int batch_lanes();
+template <typename T>
+size_t batch_smem();
+template <typename T>
+int batch_resident_blocks(int device);
+// step_items[r] = work items before window step r (r = 0..nsteps); done[] and ctl zeroed.
+// stall_plus1 > 0 is a test hook: tile (stall_plus1 - 1) never publishes its first step,
+// so the waits that depend on it run out and the launch ends with ctl->status = 1.
+template <typename T>
+cudaError_t launch_batch(const BatchInst<T>* insts, const BatchTile* tiles,
+                         const long long* step_items, int nsteps, long long total_items, int* done,
+                         BatchCtl* ctl, unsigned long long wait_ns, int stall_plus1,
+                         int resident_blocks, cudaStream_t s);
 
 // FP64 diagnostics: out[0] energy sum (before the h.x*h.y factor), out[1..5] sum of
 // squares, out[6..10] max |value| (as ordered bit patterns).  out must be zeroed first.

@@ -156,6 +156,35 @@ def test_step_n_equals_single_steps(libs, prec):
 
 
 @pytest.mark.parametrize("prec", ["f", "d"])
+def test_variants_and_segments_bitwise_equal(libs, prec):
+    """Every compiled variant and row-segment length computes the same per-node operations,
+    so results are bitwise equal; also matches the oracle (AoS and SoA far end)."""
+    lib = libs[prec]
+    for stype in (ST_AOS, ST_SOA):
+        p, g0, steps = _medium(prec, stype, 263, 171, 40)
+        outs = []
+        for var in range(5):
+            for seg in (0, 7, 33, 171):
+                t = make_task(lib, p)
+                try:
+                    assert lib.set_variant(t, var, seg) == 0
+                    assert lib.upload(t, g0.copy()) == 0
+                    assert lib.step_n(t, steps) == 0
+                    o = np.zeros_like(g0)
+                    assert lib.download(t, o) == 0
+                    outs.append(((var, seg), o))
+                finally:
+                    lib.le_free_task(t)
+        for key, o in outs[1:]:
+            assert o.tobytes() == outs[0][1].tobytes(), key
+        want = g0.copy()
+        Oracle(prec).run(want, p["nx"], p["ny"], p["dt"], p["hx"], p["hy"], p["c1"], p["c2"], p["rho"], stype, steps)
+        gd = g0.astype(np.float64)
+        Oracle("d").run(gd, p["nx"], p["ny"], p["dt"], p["hx"], p["hy"], p["c1"], p["c2"], p["rho"], stype, steps)
+        check(prec, outs[0][1], want, gd, p["nx"], p["ny"], stype, f"variants/{prec}/{stype}")
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
 def test_uniform_state_is_fixed_point(libs, prec):
     c = dict(nx=257, ny=131, hx=1.0, hy=1.0, c1=2.0, c2=1.0, rho=1.0, dt=0.25, stype=ST_AOS)
     g0 = np.tile(np.array([0.3, -0.2, 1.5, 0.25, -0.7], libs[prec].dtype), 257 * 131)
