@@ -295,20 +295,26 @@ def run_reference_arm(args):
     return 0
 
 
-def solve_plain(lib, p, per_call=True, stype=capi.ST_AOS):
+def solve_plain(lib, p, per_call=True, stype=capi.ST_AOS, timing=None):
     """One solve through the single-solve API: le_init_task, le_set_ball, le_step x steps
-    (or one le2d_step_n), download of the final fields.  Returns the fields."""
+    (or one le2d_step_n), download of the final fields.  Returns the fields; adds the
+    seconds of the step loop alone (launches until the device is idle) to timing[0]."""
     mat = lib.le_init_material(p.c1, p.c2, p.rho)
     t = lib.le_init_task(p.dt, (p.hx, p.hy), mat, (p.nx, p.ny), stype)
     try:
         for cx, cy, r, s in p.disks:
             lib.le_set_ball(t, (cx, cy), r, s)
+        assert lib.wait(t) == 0
+        t0 = time.perf_counter()
         if per_call:
             step = lib.le_step if stype == capi.ST_AOS else lib.le_step_soa
             for _ in range(p.steps):
                 step(t)
         else:
             assert lib.step_n(t, p.steps) == 0
+        assert lib.wait(t) == 0
+        if timing is not None:
+            timing[0] += time.perf_counter() - t0
         assert lib.sync_host(t) == 0 and lib.last_error(t) == 0
         return lib.grid_view(t).copy()
     finally:
@@ -342,21 +348,41 @@ def run_batched(args):
     batch_run(scale_steps=8)  # warm-up (kernels, allocations)
     ms, wall, outs = batch_run()
     # the plain loop: every instance alone, one le_step call per step
+    loop_only = [0.0]
     t0 = time.perf_counter()
     for p in probs:
-        solve_plain(lib, p, per_call=True)
+        solve_plain(lib, p, per_call=True, timing=loop_only)
     plain_s = time.perf_counter() - t0
+    loop_only_n = [0.0]
     t0 = time.perf_counter()
     for p in probs:
-        solve_plain(lib, p, per_call=False)
+        solve_plain(lib, p, per_call=False, timing=loop_only_n)
     plain_n_s = time.perf_counter() - t0
-    # accuracy: the 8 smallest instances against the FP64 library (checked against the reference)
-    worst = np.zeros(5)
-    for k in sorted(range(len(probs)), key=lambda k: probs[k].node_updates)[:8]:
+    # accuracy of the 4 smallest instances (most steps per node, most reflections): our FP32
+    # against the FP64 library (itself checked against the reference), beside the reference's
+    # own float build against its double build on the same problem (the C oracle reproduces
+    # both bit for bit), and the error relative to the norm of the whole state
+    from oracle.oracle import Oracle
+
+    acc = []
+    for k in sorted(range(len(probs)), key=lambda k: probs[k].node_updates)[:4]:
         p = probs[k]
-        ref = solve_plain(libd, p, per_call=False)
-        err = rel_l2(fields(outs[k], p.nx, p.ny, 1), fields(ref, p.nx, p.ny, 1))
-        worst = np.maximum(worst, err)
+        ref = fields(solve_plain(libd, p, per_call=False), p.nx, p.ny, 1)
+        ours = fields(outs[k], p.nx, p.ny, 1)
+        refs = {}
+        for prec in ("f", "d"):
+            o = Oracle(prec)
+            g = np.zeros(5 * p.nx * p.ny, o.dtype)
+            for d in p.disks:
+                o.set_ball(g, p.nx, p.ny, p.hx, p.hy, 1, *d)
+            o.run(g, p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, 1, p.steps)
+            refs[prec] = fields(g, p.nx, p.ny, 1)
+        state_rel = float(np.sqrt(((ours.astype(np.float64) - ref) ** 2).sum() / (ref**2).sum()))
+        acc.append({"instance": k, "nx": p.nx, "ny": p.ny, "steps": p.steps,
+                    "ours_fp32_vs_fp64_rel_l2": rel_l2(ours, ref).tolist(),
+                    "reference_float_vs_double_rel_l2": rel_l2(refs["f"], refs["d"]).tolist(),
+                    "ours_fp32_vs_fp64_state_rel_l2": state_rel})
+    worst = np.max([a["ours_fp32_vs_fp64_rel_l2"] for a in acc], axis=0)
     line = {
         "metric": "solves/s", "value": len(probs) / (ms * 1e-3), "unit": "solves/s", "n_gpus": 1,
         "workload": "batched_256: 256 FP32 solves, sides log-uniform 128-2048, c1 U[1,4], c2/c1 U[0.3,0.6], "
@@ -364,9 +390,13 @@ def run_batched(args):
         "node_updates": nu, "batched_device_s": ms * 1e-3, "batched_wall_s": wall,
         "batched_nu_s": nu / (ms * 1e-3), "window_steps": args.window,
         "plain_le_step_loop_s": plain_s, "plain_le_step_solves_s": len(probs) / plain_s,
+        "plain_le_step_loop_steps_only_s": loop_only[0],
         "plain_step_n_loop_s": plain_n_s, "plain_step_n_solves_s": len(probs) / plain_n_s,
+        "plain_step_n_loop_steps_only_s": loop_only_n[0],
         "speedup_vs_plain_le_step": plain_s / (ms * 1e-3), "speedup_vs_plain_step_n": plain_n_s / (ms * 1e-3),
-        "max_rel_l2_vs_fp64_8_smallest": worst.tolist(),
+        "speedup_vs_plain_le_step_steps_only": loop_only[0] / (ms * 1e-3),
+        "max_rel_l2_vs_fp64_4_smallest": worst.tolist(),
+        "accuracy_4_smallest": acc,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -432,13 +462,80 @@ def run_serving(args):
     return 0
 
 
+def run_precision(args):
+    """4096x4096 precision study: FP32 vs FP64 library every 500 steps up to 4000 steps,
+    FP64 energy drift, and both builds against the reference's own CPU builds after 500 steps."""
+    from oracle.oracle import Reference, aos_to_soa, fields, max_abs, rel_l2
+
+    p = workloads.precision_4096()
+    n = p.nx
+    libs = {"f": capi.Lib("f"), "d": capi.Lib("d")}
+    tasks, ics = {}, {}
+    for prec, lib in libs.items():
+        mat = lib.le_init_material(p.c1, p.c2, p.rho)
+        t = lib.le_init_task(p.dt, (p.hx, p.hy), mat, (n, n), capi.ST_AOS)
+        for cx, cy, r, s in p.disks:
+            lib.le_set_ball(t, (cx, cy), r, s)
+        assert lib.sync_host(t) == 0
+        g = lib.grid_view(t).reshape(n, n, 5)
+        vx, vy = p.noise_fields(lib.dtype)
+        g[:, :, 0] = vx
+        g[:, :, 1] = vy
+        ics[prec] = lib.grid_view(t).copy()
+        assert lib.sync_device(t) == 0
+        tasks[prec] = t
+    e0 = libs["d"].diagnostics(tasks["d"])[1]["energy"]
+    rows = []
+    snap = {}
+    for k in range(1, p.steps // 500 + 1):
+        out = {}
+        for prec, lib in libs.items():
+            assert lib.step_n(tasks[prec], 500) == 0
+            g = np.zeros(5 * n * n, lib.dtype)
+            assert lib.download(tasks[prec], g) == 0
+            out[prec] = fields(g, n, n, 1)
+            if k == 1:
+                snap[prec] = g
+        ed = libs["d"].diagnostics(tasks["d"])[1]["energy"]
+        ef = libs["f"].diagnostics(tasks["f"])[1]["energy"]
+        rows.append({"step": 500 * k, "fp32_vs_fp64_rel_l2": rel_l2(out["f"], out["d"]).tolist(),
+                     "fp32_vs_fp64_max_abs": max_abs(out["f"], out["d"]).tolist(),
+                     "fp64_energy": ed, "fp64_energy_drift": (ed - e0) / e0,
+                     "fp32_state_energy_drift": (ef - e0) / e0})
+        print(json.dumps(rows[-1]), file=sys.stderr, flush=True)
+    for prec, lib in libs.items():
+        lib.le_free_task(tasks[prec])
+    line = {"metric": "precision", "workload": "precision_4096: 4096x4096, c1=2, c2=1, rho=1, dt=0.5h/c1, "
+                                              "8 seeded disks + U(+-1e-3) noise on vx, vy", "steps": p.steps,
+            "every": 500, "rows": rows}
+    # the reference's own CPU builds (simple/, OpenMP on all host cores) from the same initial
+    # states for the first 500 steps, against the library's FP64 / FP32 results at step 500
+    if Reference.available("d") and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        for prec in ("d", "f"):
+            ref = Reference(prec)
+            g = ics[prec].copy()
+            secs = ref.run(g, n, n, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, 1, 500, threads)
+            fr = fields(g, n, n, 1)
+            fl = fields(snap[prec], n, n, 1)
+            line[f"step500_lib_{prec}_vs_reference_{prec}_rel_l2"] = rel_l2(fl, fr).tolist()
+            line[f"step500_lib_{prec}_vs_reference_{prec}_max_abs"] = max_abs(fl, fr).tolist()
+            line[f"reference_{prec}_cpu_seconds"] = secs
+            if prec == "d":
+                ref_d = fr
+        line["step500_reference_f_vs_reference_d_rel_l2"] = rel_l2(fr, ref_d).tolist()
+        line["reference_threads"] = threads
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single", choices=["single", "batched", "serving"])
+    ap.add_argument("--workload", default="single", choices=["single", "batched", "serving", "precision"])
     ap.add_argument("--window", type=int, default=256, help="steps per persistent launch (batched/serving)")
     ap.add_argument("--rates", default="10,50,200,2000", help="serving: request rates per second")
     ap.add_argument("--requests", type=int, default=48, help="serving: requests per rate")
@@ -453,6 +550,8 @@ def main():
         return run_batched(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "precision":
+        return run_precision(args)
 
     world, rank, local = dist_setup()
     backend = "nccl"

@@ -73,6 +73,16 @@ int le2d_set_variant(le_task *task, int variant, int seg_len);
 /* out[6] = {variant, columns per lane, segment rows, strips, warp tasks, blocks}. */
 int le2d_get_plan(const le_task *task, int *out);
 
+/* Autotuner: times every compiled fused-kernel variant (columns per lane, register bound,
+ * row-loop unroll) and row-segment length on a scratch state of nx x ny nodes, and keeps
+ * the fastest for the size class (nx, ny rounded up to powers of two).  Tasks created
+ * afterwards in that class use it; with LE2D_AUTOTUNE=1 le_init_task tunes a class on its
+ * first task.  out_plan (may be NULL) as le2d_get_plan; *nu_per_s (may be NULL) = the
+ * measured node-updates/s of the chosen plan. */
+int le2d_autotune(int nx, int ny, int *out_plan, double *nu_per_s);
+/* Forgets every tuned size class. */
+int le2d_autotune_reset(void);
+
 /* Simulated time and step count since le_init_task (FP64 accumulator). */
 int le2d_sim_time(const le_task *task, double *t, long long *steps);
 

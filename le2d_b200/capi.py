@@ -45,7 +45,7 @@ EXPORTS = [
     "le2d_batch_fields", "le2d_batch_receivers", "le2d_batch_diagnostics", "le2d_batch_set_wait_limit",
     "le2d_server_create", "le2d_server_destroy", "le2d_server_submit", "le2d_server_poll",
     "le2d_server_wait", "le2d_server_result", "le2d_server_times", "le2d_server_release",
-    "le2d_server_stats", "le2d_now",
+    "le2d_server_stats", "le2d_now", "le2d_autotune", "le2d_autotune_reset",
 ]
 
 LE2D_WANT_FIELDS = 0
@@ -174,6 +174,8 @@ class Lib:
         L.le2d_server_release.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
         L.le2d_server_stats.argtypes = [ctypes.c_void_p, P(le2d_server_stats_t)]
         L.le2d_now.restype = ctypes.c_double
+        L.le2d_autotune.argtypes = [ctypes.c_int, ctypes.c_int, P(ctypes.c_int), P(ctypes.c_double)]
+        L.le2d_autotune_reset.argtypes = []
 
     # --- the reference task API, same names ---
     def le_init_material(self, c1, c2, rho):
@@ -251,6 +253,18 @@ class Lib:
         if rc:
             raise RuntimeError(self.strerror(rc))
         return dict(zip(("variant", "lanes", "seg_len", "nstrips", "ntasks", "blocks"), list(out)))
+
+    def autotune(self, nx: int, ny: int):
+        out = (ctypes.c_int * 6)()
+        nus = ctypes.c_double(0.0)
+        rc = self.lib.le2d_autotune(nx, ny, out, ctypes.byref(nus))
+        if rc:
+            raise RuntimeError(self.strerror(rc))
+        plan = dict(zip(("variant", "lanes", "seg_len", "nstrips", "ntasks", "blocks"), list(out)))
+        return plan, nus.value
+
+    def autotune_reset(self) -> int:
+        return self.lib.le2d_autotune_reset()
 
     def sim_time(self, t):
         tt, st = ctypes.c_double(0.0), ctypes.c_longlong(0)

@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <unordered_map>
 
@@ -123,6 +124,114 @@ void replan(DevTask* d, int variant, int seg_len) {
 
 // Step constants from the task as it is now (the caller may change dt between steps).
 StepConsts<T> make_consts(const le_task* t) { return le2d::make_consts(t->dt, t->h, t->mat); }
+
+// ---- autotuner: fastest fused-kernel plan per size class ----
+
+struct Tuned {
+  int variant = 0, seg_len = 0;
+  double nu_s = 0.0;
+};
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, Tuned> g_tuned;
+
+int ceil_log2(int n) {
+  int k = 0;
+  while ((1 << k) < n) ++k;
+  return k;
+}
+std::pair<int, int> size_class(int nx, int ny) { return {ceil_log2(nx), ceil_log2(ny)}; }
+
+void release(DevTask* d);
+cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int method, int* cur);
+
+// Times every variant x segment length on a scratch nx x ny state (a disk of radius
+// min(nx,ny)/4 on a zero field, c1 = 2, c2 = 1, rho = 1, Courant number 0.5).
+int tune_size(int nx, int ny, Tuned* best) {
+  DevTask* d = new DevTask();
+  d->nx = nx;
+  d->ny = ny;
+  d->pitch = row_pitch(nx);
+  d->plane = d->pitch * ny;
+  d->has_device = true;
+  cudaError_t e = cudaMalloc(&d->mem, sizeof(T) * 2 * 5 * (size_t)d->plane);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    d->mem = nullptr;
+    release(d);
+    return LE2D_ENOMEM;
+  }
+  d->buf[0] = d->mem;
+  d->buf[1] = d->mem + 5 * d->plane;
+  e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&d->ev[0]);
+  if (e == cudaSuccess) e = cudaEventCreate(&d->ev[1]);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d->mem, 0, sizeof(T) * 2 * 5 * (size_t)d->plane, d->stream);
+  if (e == cudaSuccess)
+    e = le2d::launch_set_ball<T>(d->buf[0], nx, ny, d->pitch, d->plane, 1, 1, nx / 2, ny / 2,
+                                 (nx < ny ? nx : ny) / 4, 1, d->stream);
+  le_material m;
+  le_init_material(2, 1, 1, &m);
+  le_vec2 h;
+  h.x = h.y = 1;
+  const StepConsts<T> c = le2d::make_consts((real)0.25, h, m);
+  const int segs[] = {0, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+  best->nu_s = -1.0;
+  for (int v = 0; v < le2d::fused_variant_count<T>() && e == cudaSuccess; ++v) {
+    for (int s : segs) {
+      if (s > ny) continue;
+      replan(d, v, s);
+      float ms = 0.0f;
+      for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = queue_step(d, c, 0, LE2D_METHOD_FUSED, &d->cur);
+      // estimate one step, then time enough steps for ~3 ms
+      if (e == cudaSuccess) e = cudaEventRecord(d->ev[0], d->stream);
+      for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = queue_step(d, c, 0, LE2D_METHOD_FUSED, &d->cur);
+      if (e == cudaSuccess) e = cudaEventRecord(d->ev[1], d->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(d->ev[1]);
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, d->ev[0], d->ev[1]);
+      if (e != cudaSuccess) break;
+      int reps = (int)(3.0f / (ms / 3.0f + 1e-4f));
+      reps = reps < 5 ? 5 : (reps > 400 ? 400 : reps);
+      e = cudaEventRecord(d->ev[0], d->stream);
+      for (int k = 0; k < reps && e == cudaSuccess; ++k) e = queue_step(d, c, 0, LE2D_METHOD_FUSED, &d->cur);
+      if (e == cudaSuccess) e = cudaEventRecord(d->ev[1], d->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(d->ev[1]);
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, d->ev[0], d->ev[1]);
+      if (e != cudaSuccess) break;
+      const double nus = (double)nx * ny * reps / (ms * 1e-3);
+      if (nus > best->nu_s) {
+        best->nu_s = nus;
+        best->variant = v;
+        best->seg_len = s;
+      }
+    }
+  }
+  release(d);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "le2d: autotune: %s\n", cudaGetErrorString(e));
+    return LE2D_ECUDA;
+  }
+  return LE2D_OK;
+}
+
+// The tuned plan of a task's size class, tuning it first under LE2D_AUTOTUNE=1.
+bool tuned_plan(int nx, int ny, Tuned* t) {
+  if (getenv("LE2D_FUSED_VARIANT")) return false;  // an explicit variant wins
+  const auto key = size_class(nx, ny);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      *t = it->second;
+      return true;
+    }
+  }
+  const char* a = getenv("LE2D_AUTOTUNE");
+  if (!a || atoi(a) == 0) return false;
+  if (tune_size(nx, ny, t) != LE2D_OK) return false;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned[key] = *t;
+  return true;
+}
 
 bool same_consts(const StepConsts<T>& a, const StepConsts<T>& b) {
   return memcmp(&a, &b, sizeof(a)) == 0;
@@ -390,7 +499,11 @@ void le_init_task(le_task* task, const real dt, const le_vec2 h, const le_materi
         record(d, LE2D_ECUDA, "le_init_task: device setup", e);
         d->has_device = false;
       }
-      replan(d, default_variant(), 0);
+      Tuned tp;
+      if (tuned_plan(n.x, n.y, &tp))
+        replan(d, tp.variant, tp.seg_len);
+      else
+        replan(d, default_variant(), 0);
     }
   } else {
     record(d, LE2D_ENODEV, "le_init_task");
@@ -580,6 +693,38 @@ int le2d_set_variant(le_task* task, int variant, int seg_len) {
   if (variant < -1 || variant >= le2d::fused_variant_count<T>() || seg_len < 0) return LE2D_EINVAL;
   if (!d->has_device) return LE2D_ENODEV;
   replan(d, variant < 0 ? default_variant() : variant, seg_len);
+  return LE2D_OK;
+}
+
+int le2d_autotune(int nx, int ny, int* out_plan, double* nu_per_s) {
+  if (nx < 3 || ny < 3) return LE2D_EINVAL;
+  if (device_count() == 0) return LE2D_ENODEV;
+  Tuned t;
+  const int rc = tune_size(nx, ny, &t);
+  if (rc) return rc;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[size_class(nx, ny)] = t;
+  }
+  if (nu_per_s) *nu_per_s = t.nu_s;
+  if (out_plan) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    le2d::FusedPlan p = le2d::plan_fused<T>(nx, ny, t.variant,
+                                            le2d::fused_resident_warps<T>(dev, t.variant), kMinSeg);
+    out_plan[0] = t.variant;
+    out_plan[1] = p.lanes;
+    out_plan[2] = t.seg_len > 0 ? (t.seg_len < ny ? t.seg_len : ny) : p.seg_len;
+    out_plan[3] = p.nstrips;
+    out_plan[4] = p.nstrips * ((ny + out_plan[2] - 1) / out_plan[2]);
+    out_plan[5] = (out_plan[4] + p.threads / 32 - 1) / (p.threads / 32);
+  }
+  return LE2D_OK;
+}
+
+int le2d_autotune_reset(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned.clear();
   return LE2D_OK;
 }
 

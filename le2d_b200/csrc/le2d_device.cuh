@@ -11,12 +11,19 @@
 // operations).  So the kernels compute one ratio and one limited flux per face and
 // share it between the two nodes that touch the face:
 //   right-moving invariant u (w1, w3):  D_i = u_{i+1} - u_i, P_i = D_i + eps,
-//       F_i = u_i + psi(P_{i-1} / P_i) D_i,          new u_i = u_i - k (F_i - F_{i-1})
+//       F_i = u_i + psi_i D_i, psi_i = psi(P_{i-1} / P_i), new u_i = u_i - k (F_i - F_{i-1})
 //   left-moving invariant u (w2, w4):   Q_i = eps - D_i,
-//       G_i = u_i - psi(Q_i / Q_{i-1}) D_{i-1},      new u_i = u_i - k (G_i - G_{i+1})
-// with psi(r) = (1 - k)/2 * superbee(r).  The field update uses the invariant
-// changes directly, 0.5*(new u - u) = k/2 (F_{i-1} - F_i), instead of forming
-// new u and subtracting u again.
+//       G_i = u_i - psi'_i D_{i-1}, psi'_i = psi(Q_i / Q_{i-1}), new u_i = u_i - k (G_i - G_{i+1})
+// with psi(r) = (1 - k)/2 * superbee(r).
+//
+// Difference form.  The flux differences need only the face differences D:
+//   A_i = F_{i-1} - F_i = t_{i-1} - psi_i D_i,        t_i = (psi_i - 1) D_i
+//   B_i = G_{i+1} - G_i = c_i - psi'_{i+1} D_i,       c_i = D_i + psi'_i D_{i-1}
+// and D itself is formed from differences of the fields (face_differences), so the
+// update never subtracts two large invariants: in FP32 this keeps the relative
+// accuracy of small increments (e.g. residual velocities next to large static stresses)
+// that differencing the invariants loses.  The field update uses the invariant changes
+// directly, 0.5*(new u - u) = k/2 A_i (resp. k/2 B_i).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -79,16 +86,16 @@ __device__ __forceinline__ double psi(double r, double kc) {
   return kc * max3(0.0, fmin(1.0, r + r), fmin(2.0, r));
 }
 
-// Limited flux of a right-moving invariant through the face right of node i.
+// Differences of the four moving invariants across a face, formed from the differences
+// of the fields that enter them (normal velocity vn, normal stress sn, tangential
+// velocity vt, shear stress sxy) rather than by differencing the invariants.
 template <typename T>
-__device__ __forceinline__ T flux_fwd(T u, T p_left, T p_right, T d_right, T kc) {
-  return fma(psi(ratio(p_left, p_right), kc), d_right, u);
-}
-
-// Limited flux of a left-moving invariant through the face left of node i.
-template <typename T>
-__device__ __forceinline__ T flux_bwd(T u, T q_left, T q_right, T d_left, T kc) {
-  return fma(-psi(ratio(q_right, q_left), kc), d_left, u);
+__device__ __forceinline__ void face_differences(T dvn, T dsn, T dvt, T dsxy, const Sweep<T>& c,
+                                                 T& d1, T& d2, T& d3, T& d4) {
+  d1 = fma(-dsn, c.irhoc1, dvn);
+  d2 = fma(dsn, c.irhoc1, dvn);
+  d3 = fma(-dsxy, c.irhoc2, dvt);
+  d4 = fma(dsxy, c.irhoc2, dvt);
 }
 
 // Invariants of one node for a sweep along AXIS (0 = x, 1 = y).

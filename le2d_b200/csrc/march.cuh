@@ -96,56 +96,59 @@ __device__ __forceinline__ void load_row(T (&f)[NF][V], const GridRef<T>& g, int
 }
 
 // x-sweep of the V nodes of this lane (row in registers, neighbours by shuffles).
+// Face e (0..V) lies between node e-1 and node e of the lane; the neighbour lanes supply
+// the fields of nodes -1 and V and the flux terms of their edge nodes.
 template <typename T, int V>
 __device__ __forceinline__ void sweep_x_lane(T (&f)[NF][V], const Sweep<T>& c) {
   constexpr unsigned kAll = 0xffffffffu;
   const T eps = tvd_eps<T>();
-  T w[4][V];
+  // fields entering the x-invariants: vn = vx, sn = sxx, vt = vy, and sxy
+  T lf[4], rf[4];
+  {
+    const int fk[4] = {VX, SXX, VY, SXY};
 #pragma unroll
-  for (int v = 0; v < V; ++v)
-    omega<0>(f[VX][v], f[VY][v], f[SXX][v], f[SXY][v], f[SYY][v], c, w[0][v], w[1][v], w[2][v],
-             w[3][v]);
+    for (int q = 0; q < 4; ++q) {
+      lf[q] = __shfl_up_sync(kAll, f[fk[q]][V - 1], 1);
+      rf[q] = __shfl_down_sync(kAll, f[fk[q]][0], 1);
+    }
+  }
+  T d[4][V + 1];
+#pragma unroll
+  for (int e = 0; e <= V; ++e) {
+    const T nvx = e < V ? f[VX][e] : rf[0], pvx = e > 0 ? f[VX][e - 1] : lf[0];
+    const T nsx = e < V ? f[SXX][e] : rf[1], psx = e > 0 ? f[SXX][e - 1] : lf[1];
+    const T nvy = e < V ? f[VY][e] : rf[2], pvy = e > 0 ? f[VY][e - 1] : lf[2];
+    const T nxy = e < V ? f[SXY][e] : rf[3], pxy = e > 0 ? f[SXY][e - 1] : lf[3];
+    face_differences(nvx - pvx, nsx - psx, nvy - pvy, nxy - pxy, c, d[0][e], d[1][e], d[2][e],
+                     d[3][e]);
+  }
   T a[2][V], b[2][V];
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     const T kc = q ? c.kc2 : c.kc1;
-    // right-moving invariant (w1 / w3): faces e = 0..V, face e sits left of node v = e
-    {
+    {  // right-moving invariant (w1 / w3)
       const int k = 2 * q;
-      const T left = __shfl_up_sync(kAll, w[k][V - 1], 1);
-      const T right = __shfl_down_sync(kAll, w[k][0], 1);
-      T d[V + 1], pp[V + 1];
-      d[0] = w[k][0] - left;
+      T ps[V], t[V];
 #pragma unroll
-      for (int e = 1; e < V; ++e) d[e] = w[k][e] - w[k][e - 1];
-      d[V] = right - w[k][V - 1];
+      for (int v = 0; v < V; ++v) {
+        ps[v] = psi(ratio(d[k][v] + eps, d[k][v + 1] + eps), kc);
+        t[v] = fma(ps[v], d[k][v + 1], -d[k][v + 1]);
+      }
+      const T t_in = __shfl_up_sync(kAll, t[V - 1], 1);
 #pragma unroll
-      for (int e = 0; e <= V; ++e) pp[e] = d[e] + eps;
-      T fl[V];
-#pragma unroll
-      for (int v = 0; v < V; ++v) fl[v] = flux_fwd(w[k][v], pp[v], pp[v + 1], d[v + 1], kc);
-      const T f_in = __shfl_up_sync(kAll, fl[V - 1], 1);
-#pragma unroll
-      for (int v = 0; v < V; ++v) a[q][v] = (v ? fl[v - 1] : f_in) - fl[v];
+      for (int v = 0; v < V; ++v) a[q][v] = fma(-ps[v], d[k][v + 1], v ? t[v - 1] : t_in);
     }
-    // left-moving invariant (w2 / w4)
-    {
+    {  // left-moving invariant (w2 / w4)
       const int k = 2 * q + 1;
-      const T left = __shfl_up_sync(kAll, w[k][V - 1], 1);
-      const T right = __shfl_down_sync(kAll, w[k][0], 1);
-      T d[V + 1], qq[V + 1];
-      d[0] = w[k][0] - left;
+      T ps[V], h[V];
 #pragma unroll
-      for (int e = 1; e < V; ++e) d[e] = w[k][e] - w[k][e - 1];
-      d[V] = right - w[k][V - 1];
+      for (int v = 0; v < V; ++v) {
+        ps[v] = psi(ratio(eps - d[k][v + 1], eps - d[k][v]), kc);
+        h[v] = fma(-ps[v], d[k][v], d[k][v]);
+      }
+      const T h_in = __shfl_down_sync(kAll, h[0], 1);
 #pragma unroll
-      for (int e = 0; e <= V; ++e) qq[e] = eps - d[e];
-      T gl[V];
-#pragma unroll
-      for (int v = 0; v < V; ++v) gl[v] = flux_bwd(w[k][v], qq[v], qq[v + 1], d[v], kc);
-      const T g_in = __shfl_down_sync(kAll, gl[0], 1);
-#pragma unroll
-      for (int v = 0; v < V; ++v) b[q][v] = (v < V - 1 ? gl[v + 1] : g_in) - gl[v];
+      for (int v = 0; v < V; ++v) b[q][v] = fma(ps[v], d[k][v], v < V - 1 ? h[v + 1] : h_in);
     }
   }
 #pragma unroll
@@ -173,15 +176,16 @@ __device__ __forceinline__ void march_tile(const GridRef<T>& g, const StepConsts
   const T eps = tvd_eps<T>();
   const Sweep<T>& cy = c.y;
 
-  // y-pipeline state per column: u_{m-1} (4 invariants); for w1/w3: P_{m-2}, F_{m-2},
-  // A_{m-2} = F_{m-3} - F_{m-2}; for w2/w4: Q_{m-2}, D_{m-2}, G_{m-2}.
-  T um1[4][V], p2[2][V], f2[2][V], a2[2][V], q2[2][V], d2[2][V], g2[2][V];
+  // y-pipeline state per column (face j lies between rows j and j+1): the fields of row
+  // m-1 that enter the y-invariants (vy, syy, vx, sxy); for w1/w3: P_{m-2}, t_{m-2} and
+  // A_{m-1} (written out one row later); for w2/w4: Q_{m-2}, D_{m-2}, c_{m-2}.
+  T pf[4][V], p2[2][V], t2[2][V], a2[2][V], q2[2][V], d2[2][V], c2[2][V];
 #pragma unroll
   for (int v = 0; v < V; ++v) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) um1[k][v] = T(0);
+    for (int k = 0; k < 4; ++k) pf[k][v] = T(0);
 #pragma unroll
-    for (int q = 0; q < 2; ++q) p2[q][v] = f2[q][v] = a2[q][v] = q2[q][v] = d2[q][v] = g2[q][v] = T(0);
+    for (int q = 0; q < 2; ++q) p2[q][v] = t2[q][v] = a2[q][v] = q2[q][v] = d2[q][v] = c2[q][v] = T(0);
   }
 
   T nxt[NF][V];
@@ -206,32 +210,34 @@ __device__ __forceinline__ void march_tile(const GridRef<T>& g, const StepConsts
     T a_out[2][V], b_out[2][V];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-      T u[4];
-      omega<1>(f[VX][v], f[VY][v], f[SXX][v], f[SXY][v], f[SYY][v], cy, u[0], u[1], u[2], u[3]);
+      // D_{m-1} of the four invariants from the field differences of rows m-1 and m
+      T d[4];
+      face_differences(f[VY][v] - pf[0][v], f[SYY][v] - pf[1][v], f[VX][v] - pf[2][v],
+                       f[SXY][v] - pf[3][v], cy, d[0], d[1], d[2], d[3]);
+      pf[0][v] = f[VY][v];
+      pf[1][v] = f[SYY][v];
+      pf[2][v] = f[VX][v];
+      pf[3][v] = f[SXY][v];
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const T kc = q ? cy.kc2 : cy.kc1;
-        {  // right-moving: F_{m-1}, A_{m-1}
-          const int k = 2 * q;
-          const T d1 = u[k] - um1[k][v];
-          const T p1 = d1 + eps;
-          const T f1 = flux_fwd(um1[k][v], p2[q][v], p1, d1, kc);
+        {  // right-moving: psi_{m-1}, A_{m-1} = t_{m-2} - psi_{m-1} D_{m-1}, t_{m-1}
+          const T dd = d[2 * q];
+          const T p1 = dd + eps;
+          const T ps = psi(ratio(p2[q][v], p1), kc);
           a_out[q][v] = a2[q][v];
-          a2[q][v] = f2[q][v] - f1;
-          f2[q][v] = f1;
+          a2[q][v] = fma(-ps, dd, t2[q][v]);
+          t2[q][v] = fma(ps, dd, -dd);
           p2[q][v] = p1;
-          um1[k][v] = u[k];
         }
-        {  // left-moving: G_{m-1}, B_{m-2}
-          const int k = 2 * q + 1;
-          const T d1 = u[k] - um1[k][v];
-          const T q1 = eps - d1;
-          const T g1 = flux_bwd(um1[k][v], q2[q][v], q1, d2[q][v], kc);
-          b_out[q][v] = g1 - g2[q][v];
-          g2[q][v] = g1;
+        {  // left-moving: psi'_{m-1}, B_{m-2} = c_{m-2} - psi'_{m-1} D_{m-2}, c_{m-1}
+          const T dd = d[2 * q + 1];
+          const T q1 = eps - dd;
+          const T ps = psi(ratio(q1, q2[q][v]), kc);
+          b_out[q][v] = fma(-ps, d2[q][v], c2[q][v]);
+          c2[q][v] = fma(ps, d2[q][v], dd);
+          d2[q][v] = dd;
           q2[q][v] = q1;
-          d2[q][v] = d1;
-          um1[k][v] = u[k];
         }
       }
     }

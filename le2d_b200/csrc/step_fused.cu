@@ -46,11 +46,11 @@ template <> struct VariantCfg<float, 1> { static constexpr int V = 4, MINB = 1, 
 template <> struct VariantCfg<float, 2> { static constexpr int V = 2, MINB = 4, UNROLL = 1; };
 template <> struct VariantCfg<float, 3> { static constexpr int V = 2, MINB = 4, UNROLL = 2; };
 template <> struct VariantCfg<float, 4> { static constexpr int V = 4, MINB = 3, UNROLL = 2; };
-template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 3, UNROLL = 1; };
-template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 4, UNROLL = 1; };
+template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 2, UNROLL = 1; };
+template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 3, UNROLL = 1; };
 template <> struct VariantCfg<double, 2> { static constexpr int V = 1, MINB = 4, UNROLL = 1; };
 template <> struct VariantCfg<double, 3> { static constexpr int V = 1, MINB = 4, UNROLL = 2; };
-template <> struct VariantCfg<double, 4> { static constexpr int V = 1, MINB = 5, UNROLL = 2; };
+template <> struct VariantCfg<double, 4> { static constexpr int V = 1, MINB = 3, UNROLL = 2; };
 constexpr int kVariants = 5;
 
 template <typename T, int VAR>
