@@ -95,6 +95,24 @@ typedef struct {
 } le2d_diag_t;
 int le2d_diagnostics(le_task *task, le2d_diag_t *out);
 
+/* The same diagnostics for callers that cannot allocate device memory -- hosts that
+ * budget every byte of device memory up front (a fixed serving arena), or time loops
+ * where a cudaMalloc/cudaFree would synchronise the device.  No counterpart in the
+ * reference (which has no device and no diagnostics).  Needs no task and allocates
+ * nothing: d_state is the caller's SoA state on the current device (field k, row j,
+ * column i at d_state[k*plane + j*pitch + i]; pitch >= nx, plane >= pitch*ny), `stream`
+ * a cudaStream_t (NULL = legacy default stream), result in *out.  Its scratch is a
+ * library-static device array of per-row partial sums (reduced in a fixed order, so
+ * repeated calls give identical results) for at most LE2D_DIAG_NOALLOC_MAX_ROWS rows
+ * (larger grids: LE2D_EINVAL); every GPU that loads the library holds it (~1.4 MB)
+ * until exit.  All calls share it: calls whose kernels overlap on the GPU race.  The
+ * first call on a device looks up the array's device address; make that first call
+ * before any stream capture. */
+#define LE2D_DIAG_NOALLOC_MAX_ROWS 16384
+int le2d_diagnostics_noalloc(const real *d_state, int nx, int ny, long long pitch,
+			     long long plane, real hx, real hy, real c1, real c2, real rho,
+			     void *stream, le2d_diag_t *out);
+
 /* ---- Batched solves ------------------------------------------------------------------
  * Many independent solves of different sizes, materials, initial conditions and step
  * counts, advanced together by one persistent kernel over a tile work list (each tile

@@ -45,8 +45,10 @@ EXPORTS = [
     "le2d_batch_fields", "le2d_batch_receivers", "le2d_batch_diagnostics", "le2d_batch_set_wait_limit",
     "le2d_server_create", "le2d_server_destroy", "le2d_server_submit", "le2d_server_poll",
     "le2d_server_wait", "le2d_server_result", "le2d_server_times", "le2d_server_release",
-    "le2d_server_stats", "le2d_now", "le2d_autotune", "le2d_autotune_reset",
+    "le2d_server_stats", "le2d_now", "le2d_diagnostics_noalloc", "le2d_autotune", "le2d_autotune_reset",
 ]
+
+LE2D_DIAG_NOALLOC_MAX_ROWS = 16384
 
 LE2D_WANT_FIELDS = 0
 LE2D_WANT_RECEIVERS = 1
@@ -176,6 +178,9 @@ class Lib:
         L.le2d_now.restype = ctypes.c_double
         L.le2d_autotune.argtypes = [ctypes.c_int, ctypes.c_int, P(ctypes.c_int), P(ctypes.c_double)]
         L.le2d_autotune_reset.argtypes = []
+        L.le2d_diagnostics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
+                                               ctypes.c_longlong, R, R, R, R, R, ctypes.c_void_p,
+                                               P(self.le2d_diag_t)]
 
     # --- the reference task API, same names ---
     def le_init_material(self, c1, c2, rho):
@@ -274,6 +279,14 @@ class Lib:
     def diagnostics(self, t):
         d = self.le2d_diag_t()
         rc = self.lib.le2d_diagnostics(ctypes.byref(t), ctypes.byref(d))
+        return rc, {"energy": d.energy, "sumsq": list(d.sumsq), "maxabs": list(d.maxabs)}
+
+    def diagnostics_noalloc(self, d_state: int, nx: int, ny: int, pitch: int, plane: int, hx, hy, c1, c2, rho,
+                            stream: int = 0):
+        """Diagnostics of a device state the caller holds (device pointer `d_state`)."""
+        d = self.le2d_diag_t()
+        rc = self.lib.le2d_diagnostics_noalloc(d_state, nx, ny, pitch, plane, hx, hy, c1, c2, rho,
+                                               stream or None, ctypes.byref(d))
         return rc, {"energy": d.energy, "sumsq": list(d.sumsq), "maxabs": list(d.maxabs)}
 
     def device_layout(self, t):
