@@ -12,7 +12,9 @@ Our arm (default) prints one JSON line with
   e2e       nu/s through the C ABI with host buffers: upload of the initial state
             from page-locked memory, 1000 steps, download of the final fields,
   roofline  the fused step kernel against the measured HBM copy bandwidth,
-            40 algorithmic bytes per node-update in FP32 (read + write of 5 fields),
+            40 algorithmic bytes per node-update in FP32 (read + write of 5 fields);
+            a launch of temporal-block depth 2 advances every node two steps, so its
+            algorithmic bytes are 2 x 40 B per node while it moves about half of that,
   cpu_baseline  the reference's own simple/ solver (oracle/_ref) on the host cores,
   fp64      the same measurement for the FP64 library (80 B per node-update).
 Under torchrun each rank solves its own instance (independent solves, weak scaling);
@@ -202,7 +204,7 @@ def measure_ours(lib, prec, p, steps, warmup, dist, backend, device):
         dist_barrier(dist)
         e2e_slow = dist_max(dist, e2e_s, backend)
         assert np.isfinite(host_out).all()
-        return slow_ms, clocks, e2e_slow, ic
+        return slow_ms, clocks, e2e_slow, ic, lib.get_plan(t)
     finally:
         lib.le_free_task(t)
         lib.le_free_task(e2e_t)
@@ -529,13 +531,49 @@ def run_precision(args):
     return 0
 
 
+def run_precision_reference(args):
+    """CPU only: the reference's own float and double builds (simple/, OpenMP on all host
+    cores) on the 4096x4096 precision workload, relative L2 and max-abs of float against
+    double every 500 steps up to 4000 -- the reference's own FP32 divergence curve beside
+    which `--workload precision` reports the library's (takes ~1 h on 8 cores)."""
+    from oracle.oracle import Oracle, Reference, fields, max_abs, rel_l2
+
+    p = workloads.precision_4096(steps=args.time_steps or 4000)
+    n = p.nx
+    threads = os.cpu_count() or 1
+    grids = {}
+    for prec in ("f", "d"):
+        o = Oracle(prec)
+        g = np.zeros(5 * n * n, o.dtype)
+        for cx, cy, r, s in p.disks:
+            o.set_ball(g, n, n, p.hx, p.hy, 1, cx, cy, r, s)
+        vx, vy = p.noise_fields(o.dtype)
+        a = g.reshape(n, n, 5)
+        a[:, :, 0] = vx
+        a[:, :, 1] = vy
+        grids[prec] = g
+    refs = {prec: Reference(prec) for prec in ("f", "d")}
+    rows = []
+    for k in range(1, p.steps // 500 + 1):
+        secs = {}
+        for prec in ("f", "d"):
+            secs[prec] = refs[prec].run(grids[prec], n, n, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, 1, 500, threads)
+        ff, fd = fields(grids["f"], n, n, 1), fields(grids["d"], n, n, 1)
+        rows.append({"step": 500 * k, "reference_f_vs_d_rel_l2": rel_l2(ff, fd).tolist(),
+                     "reference_f_vs_d_max_abs": max_abs(ff, fd).tolist(), "seconds": secs})
+        print(json.dumps(rows[-1]), file=sys.stderr, flush=True)
+    print(json.dumps({"metric": "precision-reference", "threads": threads, "rows": rows}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single", choices=["single", "batched", "serving", "precision"])
+    ap.add_argument("--workload", default="single",
+                    choices=["single", "batched", "serving", "precision", "precision-reference"])
     ap.add_argument("--window", type=int, default=256, help="steps per persistent launch (batched/serving)")
     ap.add_argument("--rates", default="10,50,200,2000", help="serving: request rates per second")
     ap.add_argument("--requests", type=int, default=48, help="serving: requests per rate")
@@ -552,6 +590,8 @@ def main():
         return run_serving(args)
     if args.workload == "precision":
         return run_precision(args)
+    if args.workload == "precision-reference":
+        return run_precision_reference(args)
 
     world, rank, local = dist_setup()
     backend = "nccl"
@@ -561,13 +601,19 @@ def main():
     p = workloads.single_8192() if args.time_steps is None else workloads.single_8192(args.time_steps)
     peak, peak_kind = measured_peaks()
 
-    slow_ms, clocks, e2e_s, ic = measure_ours(lib, "f", p, args.steps, args.warmup, dist, backend, local)
+    slow_ms, clocks, e2e_s, ic, plan = measure_ours(lib, "f", p, args.steps, args.warmup, dist, backend, local)
     nu = p.node_updates * args.steps * world
     value = nu / (slow_ms * 1e-3)
-    launches = args.steps * p.steps  # one fused-step kernel per time step
+    depth = plan["depth"]  # time steps per fused-kernel launch (temporal blocking)
+    per_solve = p.steps // depth + p.steps % depth
+    launches = args.steps * per_solve
     avg_launch_s = slow_ms * 1e-3 / launches
-    achieved = BYTES_PER_NU["f"] * p.nodes / avg_launch_s / 1e9
-    traffic = profiled_traffic().get("fused_step_f32_8192")
+    # algorithmic bytes: one read + one write of the state per node-update, depth node-updates
+    # per node and launch
+    alg_bytes = BYTES_PER_NU["f"] * p.nodes * depth
+    achieved = alg_bytes / avg_launch_s / 1e9
+    kname = f"fused_step_kernel<float, V={plan['lanes']}, depth={depth}>"
+    traffic = profiled_traffic().get(f"fused_step_f32_8192_depth{depth}")
     line = {
         "metric": "node-updates/s", "value": value, "unit": "node-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": slow_ms / args.steps,
@@ -579,25 +625,28 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,
                      "traffic": traffic.get("bytes_per_launch") if traffic else None,
-                     "kernel": "fused_step_kernel<float,4>",
-                     "algorithmic_bytes_per_launch": BYTES_PER_NU["f"] * p.nodes},
+                     "kernel": kname, "variant": plan["variant"], "seg_len": plan["seg_len"],
+                     "algorithmic_bytes_per_launch": alg_bytes},
         "e2e": {"value": nu / e2e_s, "unit": "node-updates/s",
                 "h2d_bytes_per_step": int(ic.nbytes), "d2h_bytes_per_step": int(ic.nbytes)},
-        "gpu_launches": launches,
+        "gpu_launches": launches,  # fused-kernel launches in the timed region
         "clocks": clocks,
     }
     if not args.no_fp64:
         libd = capi.Lib("d")
         assert libd.set_device(local) == 0
         ksteps = min(args.steps, 2)
-        d_ms, d_clk, d_e2e, d_ic = measure_ours(libd, "d", p, ksteps, min(args.warmup, 3), dist, backend, local)
+        d_ms, d_clk, d_e2e, d_ic, d_plan = measure_ours(libd, "d", p, ksteps, min(args.warmup, 3), dist, backend,
+                                                         local)
         d_nu = p.node_updates * ksteps * world
-        d_avg = d_ms * 1e-3 / (ksteps * p.steps)
-        d_ach = BYTES_PER_NU["d"] * p.nodes / d_avg / 1e9
+        d_depth = d_plan["depth"]
+        d_avg = d_ms * 1e-3 / (ksteps * (p.steps // d_depth + p.steps % d_depth))
+        d_ach = BYTES_PER_NU["d"] * p.nodes * d_depth / d_avg / 1e9
         line["fp64"] = {"value": d_nu / (d_ms * 1e-3), "unit": "node-updates/s", "steps": ksteps,
                         "ms_per_step": d_ms / ksteps, "e2e": d_nu / d_e2e,
                         "roofline": {"bound": "hbm", "achieved": d_ach, "peak": peak, "unit": "GB/s",
-                                     "frac": d_ach / peak, "kernel": "fused_step_kernel<double,2>"},
+                                     "frac": d_ach / peak,
+                                     "kernel": f"fused_step_kernel<double, V={d_plan['lanes']}, depth={d_depth}>"},
                         "clocks": d_clk}
     if rank == 0 and not args.no_cpu:
         cb = cpu_reference_sample(p)

@@ -67,10 +67,13 @@ int le2d_step_n_timed(le_task *task, int nsteps, float *ms);
 #define LE2D_METHOD_SPLIT 1
 int le2d_set_method(le_task *task, int method);
 
-/* Fused-kernel variant (columns per lane / register bound / unroll; -1 = default) and row
- * segment length (0 = fill the device once) for this task's grid. */
+/* Fused-kernel variant (columns per lane / register bound / input-ring depth / temporal-block
+ * depth; -1 = default) and row segment length (0 = fill the device once) for this task's
+ * grid.  A variant of temporal-block depth 2 advances two steps per launch; odd step counts
+ * and le_step_soa then take single steps. */
 int le2d_set_variant(le_task *task, int variant, int seg_len);
-/* out[6] = {variant, columns per lane, segment rows, strips, warp tasks, blocks}. */
+/* out[7] = {variant, columns per lane, segment rows, strips, warp tasks, blocks,
+ * temporal-block depth}. */
 int le2d_get_plan(const le_task *task, int *out);
 
 /* Autotuner: times every compiled fused-kernel variant (columns per lane, register bound,

@@ -252,21 +252,22 @@ class Lib:
     def set_variant(self, t, variant: int, seg_len: int = 0) -> int:
         return self.lib.le2d_set_variant(ctypes.byref(t), variant, seg_len)
 
+    PLAN_KEYS = ("variant", "lanes", "seg_len", "nstrips", "ntasks", "blocks", "depth")
+
     def get_plan(self, t) -> dict:
-        out = (ctypes.c_int * 6)()
+        out = (ctypes.c_int * len(self.PLAN_KEYS))()
         rc = self.lib.le2d_get_plan(ctypes.byref(t), out)
         if rc:
             raise RuntimeError(self.strerror(rc))
-        return dict(zip(("variant", "lanes", "seg_len", "nstrips", "ntasks", "blocks"), list(out)))
+        return dict(zip(self.PLAN_KEYS, list(out)))
 
     def autotune(self, nx: int, ny: int):
-        out = (ctypes.c_int * 6)()
+        out = (ctypes.c_int * len(self.PLAN_KEYS))()
         nus = ctypes.c_double(0.0)
         rc = self.lib.le2d_autotune(nx, ny, out, ctypes.byref(nus))
         if rc:
             raise RuntimeError(self.strerror(rc))
-        plan = dict(zip(("variant", "lanes", "seg_len", "nstrips", "ntasks", "blocks"), list(out)))
-        return plan, nus.value
+        return dict(zip(self.PLAN_KEYS, list(out))), nus.value
 
     def autotune_reset(self) -> int:
         return self.lib.le2d_autotune_reset()

@@ -25,7 +25,7 @@ namespace le2d {
 namespace {
 
 constexpr int kWarps = 4;
-constexpr int kLanes = 4;  // columns per lane (FP32)
+constexpr int kNpf = 2;  // input-ring depth of the march (one row in flight ahead)
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
                  unsigned long long wait_ns, int stall_plus1) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
-  T* ring = reinterpret_cast<T*>(smem_raw) + (threadIdx.x >> 5) * (3 * NF * 32 * V);
+  T* ring = reinterpret_cast<T*>(smem_raw) + (threadIdx.x >> 5) * march::warp_smem_elems<T, V, kNpf>();
   const long long total = step_items[nsteps];
   int r = 0;
   while (true) {
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
     const long long step_after = I.abs_step0 + r + 1;  // absolute step count after this step
     if (I.trace != nullptr && step_after % I.trace_every == 0)
       tap = march::RowTap<T>{I.trace + (step_after / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
-    march::march_tile<T, V, 1, true, true>(g, I.c, bt.strip, y0, y1, ring, tap);
+    march::march_tile<T, V, kNpf, true, true>(g, I.c, bt.strip, y0, y1, ring, tap);
     __syncwarp();
     const int tile_id = I.tile_base + bt.seg * I.nstrips + bt.strip;
     if (lane == 0 && !(r == 0 && tile_id == stall_plus1 - 1)) {
@@ -126,12 +126,17 @@ template <typename T>
 int batch_lanes() { return BatchKernelOf<T>::V; }
 
 template <typename T>
-size_t batch_smem() { return (size_t)kWarps * 3 * NF * 32 * BatchKernelOf<T>::V * sizeof(T); }
+size_t batch_smem() {
+  return (size_t)kWarps * march::warp_smem_elems<T, BatchKernelOf<T>::V, kNpf>() * sizeof(T);
+}
 
 template <typename T>
 int batch_resident_blocks(int device) {
   using K = BatchKernelOf<T>;
   int sms = 0, per_sm = 0;
+  // dynamic shared memory above 48 KB is opted into once (before any launch or capture)
+  cudaFuncSetAttribute(batch_kernel<T, K::V, K::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)batch_smem<T>());
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<T, K::V, K::MINB>,
                                                     kWarps * 32, batch_smem<T>()) != cudaSuccess)

@@ -52,6 +52,7 @@ struct DevTask {
   int err = LE2D_OK;
   int method = LE2D_METHOD_FUSED;
   FusedPlan plan;
+  FusedPlan plan1;  // depth-1 plan for single steps when `plan` has depth 2
   long long steps = 0;
   double sim_time = 0.0;
   // CUDA graph of kGraphSteps steps starting from buffer graph_cur.
@@ -93,13 +94,17 @@ DevTask* lookup(const le_task* task) {
 
 long long row_pitch(int nx) { return le2d::row_pitch_elems(nx); }
 
-// Fused-kernel variant used for new tasks: LE2D_FUSED_VARIANT if set, else 0.
+// Fused-kernel variant used for new tasks: LE2D_FUSED_VARIANT if set, else the fastest
+// measured on large grids (FP32: two steps per launch, 2 columns per lane, 16 warps per SM;
+// FP64: one step per launch, 2 columns per lane -- two-step FP64 tiles need twice the
+// registers and run at 8 warps per SM).
 int default_variant() {
   static int v = -2;
   if (v == -2) {
+    const int dflt = sizeof(T) == 4 ? 7 : 0;
     const char* e = getenv("LE2D_FUSED_VARIANT");
-    v = e ? atoi(e) : 0;
-    if (v < 0 || v >= le2d::fused_variant_count<T>()) v = 0;
+    v = e ? atoi(e) : dflt;
+    if (v < 0 || v >= le2d::fused_variant_count<T>()) v = dflt;
   }
   return v;
 }
@@ -118,6 +123,11 @@ void replan(DevTask* d, int variant, int seg_len) {
     p.blocks = (p.ntasks + wpb - 1) / wpb;
   }
   d->plan = p;
+  d->plan1 = p;
+  if (p.depth != 1) {  // odd remainders and le_step_soa run single steps
+    const int v = sizeof(T) == 4 ? 2 : 0;  // the fastest one-step variant
+    d->plan1 = le2d::plan_fused<T>(d->nx, d->ny, v, le2d::fused_resident_warps<T>(dev, v), kMinSeg);
+  }
   if (d->graph) cudaGraphExecDestroy(d->graph);
   d->graph = nullptr;
 }
@@ -142,7 +152,8 @@ int ceil_log2(int n) {
 std::pair<int, int> size_class(int nx, int ny) { return {ceil_log2(nx), ceil_log2(ny)}; }
 
 void release(DevTask* d);
-cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int method, int* cur);
+cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int method, int* cur,
+                       int max_steps, int* done);
 
 // Times every variant x segment length on a scratch nx x ny state (a disk of radius
 // min(nx,ny)/4 on a zero field, c1 = 2, c2 = 1, rho = 1, Courant number 0.5).
@@ -181,23 +192,28 @@ int tune_size(int nx, int ny, Tuned* best) {
       if (s > ny) continue;
       replan(d, v, s);
       float ms = 0.0f;
-      for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = queue_step(d, c, 0, LE2D_METHOD_FUSED, &d->cur);
-      // estimate one step, then time enough steps for ~3 ms
+      int steps = 0;
+      for (int k = 0; k < 2 && e == cudaSuccess; ++k)
+        e = queue_step(d, c, 0, LE2D_METHOD_FUSED, &d->cur, 2, &steps);
+      // estimate one launch, then time enough launches for ~3 ms
       if (e == cudaSuccess) e = cudaEventRecord(d->ev[0], d->stream);
-      for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = queue_step(d, c, 0, LE2D_METHOD_FUSED, &d->cur);
+      for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+        e = queue_step(d, c, 0, LE2D_METHOD_FUSED, &d->cur, 2, &steps);
       if (e == cudaSuccess) e = cudaEventRecord(d->ev[1], d->stream);
       if (e == cudaSuccess) e = cudaEventSynchronize(d->ev[1]);
       if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, d->ev[0], d->ev[1]);
       if (e != cudaSuccess) break;
       int reps = (int)(3.0f / (ms / 3.0f + 1e-4f));
       reps = reps < 5 ? 5 : (reps > 400 ? 400 : reps);
+      steps = 0;
       e = cudaEventRecord(d->ev[0], d->stream);
-      for (int k = 0; k < reps && e == cudaSuccess; ++k) e = queue_step(d, c, 0, LE2D_METHOD_FUSED, &d->cur);
+      for (int k = 0; k < reps && e == cudaSuccess; ++k)
+        e = queue_step(d, c, 0, LE2D_METHOD_FUSED, &d->cur, 2, &steps);
       if (e == cudaSuccess) e = cudaEventRecord(d->ev[1], d->stream);
       if (e == cudaSuccess) e = cudaEventSynchronize(d->ev[1]);
       if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, d->ev[0], d->ev[1]);
       if (e != cudaSuccess) break;
-      const double nus = (double)nx * ny * reps / (ms * 1e-3);
+      const double nus = (double)nx * ny * steps / (ms * 1e-3);
       if (nus > best->nu_s) {
         best->nu_s = nus;
         best->variant = v;
@@ -279,21 +295,28 @@ int ensure_host_current(DevTask* d, le_task* task) {
   return LE2D_OK;
 }
 
-// Queues one step from buf[cur]; the fused kernel writes buf[cur^1] and flips cur,
-// the split scheme sweeps x into buf[cur^1] and y back into buf[cur].
-cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int method, int* cur) {
+// Queues one launch of at most max_steps (>= 1) steps from buf[cur] and adds the steps it
+// makes to *done.  The fused kernel writes buf[cur^1] and flips cur -- two steps when the
+// plan has temporal-block depth 2 and two are wanted (clamped ends only), else one; the
+// split scheme sweeps x into buf[cur^1] and y back into buf[cur].
+cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int method, int* cur,
+                       int max_steps, int* done) {
   T* a = d->buf[*cur];
   T* b = d->buf[*cur ^ 1];
   if (method == LE2D_METHOD_SPLIT) {
     cudaError_t e = le2d::launch_split_sweep<T>(0, a, b, d->nx, d->ny, d->pitch, d->plane, c.x,
                                                 c.x.k1, c.x.k2, 0, d->stream);
     if (e != cudaSuccess) return e;
+    *done += 1;
     return le2d::launch_split_sweep<T>(1, b, a, d->nx, d->ny, d->pitch, d->plane, c.y, c.y.k1,
                                        c.y.k2, far_rot, d->stream);
   }
+  const bool two = d->plan.depth == 2 && max_steps >= 2 && !far_rot;
+  const FusedPlan& pl = two ? d->plan : d->plan1;
   cudaError_t e = le2d::launch_fused_step<T>(a, b, d->nx, d->ny, d->pitch, d->plane, c, far_rot,
-                                             d->plan, d->stream);
+                                             pl, d->stream);
   *cur ^= 1;
+  *done += pl.depth;
   return e;
 }
 
@@ -330,7 +353,8 @@ int run_steps(le_task* task, int nsteps, bool soa_entry, float* ms) {
       e = cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal);
       if (e != cudaSuccess) return record(d, LE2D_ECUDA, "graph capture", e);
       int cur = d->cur;
-      for (int s = 0; s < kGraphSteps && e == cudaSuccess; ++s) e = queue_step(d, c, far_rot, d->method, &cur);
+      for (int s = 0; s < kGraphSteps && e == cudaSuccess;)
+        e = queue_step(d, c, far_rot, d->method, &cur, kGraphSteps - s, &s);
       cudaError_t e2 = cudaStreamEndCapture(d->stream, &g);
       if (e != cudaSuccess || e2 != cudaSuccess)
         return record(d, LE2D_ECUDA, "graph capture", e != cudaSuccess ? e : e2);
@@ -346,9 +370,11 @@ int run_steps(le_task* task, int nsteps, bool soa_entry, float* ms) {
     if (e != cudaSuccess) return record(d, LE2D_ECUDA, "graph launch", e);
     left -= kGraphSteps;
   }
-  for (; left > 0; --left) {
-    e = queue_step(d, c, far_rot, d->method, &d->cur);
+  while (left > 0) {
+    int done = 0;
+    e = queue_step(d, c, far_rot, d->method, &d->cur, left, &done);
     if (e != cudaSuccess) return record(d, LE2D_ECUDA, "step kernel launch", e);
+    left -= done;
   }
   if (ms) {
     e = cudaEventRecord(d->ev[1], d->stream);
@@ -718,6 +744,7 @@ int le2d_autotune(int nx, int ny, int* out_plan, double* nu_per_s) {
     out_plan[3] = p.nstrips;
     out_plan[4] = p.nstrips * ((ny + out_plan[2] - 1) / out_plan[2]);
     out_plan[5] = (out_plan[4] + p.threads / 32 - 1) / (p.threads / 32);
+    out_plan[6] = p.depth;
   }
   return LE2D_OK;
 }
@@ -738,6 +765,7 @@ int le2d_get_plan(const le_task* task, int* out) {
   out[3] = d->plan.nstrips;
   out[4] = d->plan.ntasks;
   out[5] = d->plan.blocks;
+  out[6] = d->plan.depth;
   return LE2D_OK;
 }
 

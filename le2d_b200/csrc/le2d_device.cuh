@@ -59,13 +59,26 @@ __device__ __forceinline__ double tvd_eps<double>() { return 1e-6; }
 // Slope ratio a / b.  FP32: hardware reciprocal (rcp.approx, <= 1 ulp) times a;
 // for b = +-0 it gives +-inf (a != 0) or NaN (a = 0) like the division does, and the
 // limiter maps those exactly as the reference (superbee(+-inf) = 2 / 0, superbee(NaN) = 2).
-// FP64: IEEE division.
 __device__ __forceinline__ float ratio(float a, float b) {
   float r;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
   return a * r;
 }
-__device__ __forceinline__ double ratio(double a, double b) { return a / b; }
+// FP64: Newton-Raphson division.  The hardware reciprocal estimate y0 (about 23 bits) is
+// refined by two Newton steps y <- y + y (1 - b y) (each doubles the correct bits), and the
+// quotient q = a y by one correction with its FMA residual, q + (a - b q) y (Markstein's
+// final step): within an ulp of the IEEE quotient, at about half the instructions of the
+// full division sequence.  For b = +-0 the estimate is +-inf and for b = +-inf it is 0; in
+// both cases a * y0 already equals a / b (+-inf / NaN, or 0), so that product is returned.
+__device__ __forceinline__ double ratio(double a, double b) {
+  double y0;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(b));
+  double y = fma(y0, fma(-b, y0, 1.0), y0);
+  y = fma(y, fma(-b, y, 1.0), y);
+  const double q = a * y;
+  const double r = fma(fma(-b, q, a), y, q);
+  return (y0 == 0.0 || isinf(y0)) ? a * y0 : r;
+}
 
 __device__ __forceinline__ float max3(float a, float b, float c) {
   float d;

@@ -18,6 +18,7 @@ __host__ __device__ constexpr int strip_cols(int lanes) { return (32 - 2 * halo_
 
 struct FusedPlan {
   int variant = 0, lanes = 0;
+  int depth = 1;  // temporal-block depth: steps per launch
   int nstrips = 0, seg_len = 0, nsegs = 0, ntasks = 0;
   int blocks = 0, threads = 0;
   size_t smem = 0;
@@ -28,6 +29,8 @@ template <typename T>
 int fused_variant_count();
 template <typename T>
 int fused_variant_lanes(int variant);
+template <typename T>
+int fused_variant_depth(int variant);
 
 template <typename T>
 FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_seg);
@@ -36,7 +39,8 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
 template <typename T>
 int fused_resident_warps(int device, int variant);
 
-// One fused time step src -> dst.  far_rot selects the le_step_soa far-end rows.
+// One fused launch src -> dst: plan.depth time steps.  far_rot selects the le_step_soa
+// far-end rows (depth-1 plans only).
 template <typename T>
 cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pitch,
                               long long plane, const StepConsts<T>& c, int far_rot,

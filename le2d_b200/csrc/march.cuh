@@ -157,101 +157,301 @@ __device__ __forceinline__ void sweep_x_lane(T (&f)[NF][V], const Sweep<T>& c) {
                        a[1][v], b[1][v], c);
 }
 
+// Shared memory of one warp: NPF rows of raw input (filled by cp.async, NPF-1 rows ahead)
+// and 3 x-swept rows, each NF fields x 32*V columns.
+template <typename T, int V, int NPF>
+__host__ __device__ constexpr int warp_smem_elems() {
+  return (3 + NPF) * NF * 32 * V;
+}
+
+// Asynchronous global -> shared copy of one lane's V columns of one field (L2 only for
+// 16-byte pieces, so it is also safe when other warps of the launch wrote the source).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(gmem), "n"(BYTES)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Starts copying source row `row` into this lane's slot of the input ring.  Strips that
+// reach past the grid edge load their clamped columns synchronously instead.
+template <typename T, int V, bool COHERENT>
+__device__ __forceinline__ void fetch_row(T* slot, const GridRef<T>& g, int row, int col0,
+                                          bool interior) {
+  constexpr int kIn = 32 * V;
+  const T* base = g.src + (long long)row * g.pitch;
+  if (interior) {
+#pragma unroll
+    for (int k = 0; k < NF; ++k) cp_async<V * (int)sizeof(T)>(slot + k * kIn, base + k * g.plane + col0);
+  } else {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const int cc = min(max(col0 + v, 0), g.nx - 1);
+#pragma unroll
+      for (int k = 0; k < NF; ++k) slot[k * kIn + v] = load_state<COHERENT>(base + k * g.plane + cc);
+    }
+  }
+  cp_async_commit();
+}
+
+// The per-column y-pipeline.  Row m arrives x-swept; with the fields of row m-1 it gives
+// the face differences D_{m-1}.  left() advances the left-moving invariants (B_{m-2},
+// c_{m-1}), apply() adds the increments of row m-2 to its fields, right() advances the
+// right-moving ones (A_{m-1}, t_{m-1}).  Face j lies between rows j and j+1.  State: for
+// w1/w3 P_{m-2}, t_{m-2}, A_{m-2}; for w2/w4 Q_{m-2}, D_{m-2}, c_{m-2}.
+template <typename T, int V>
+struct YPipe {
+  T p2[2][V], t2[2][V], a2[2][V], q2[2][V], d2[2][V], c2[2][V];
+  T dfw[2][V], bo[2][V];
+
+  __device__ __forceinline__ void init() {
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) p2[q][v] = t2[q][v] = a2[q][v] = q2[q][v] = d2[q][v] = c2[q][v] = T(0);
+  }
+
+  __device__ __forceinline__ void left(const T (&f)[NF][V], const T (&pvy)[V], const T (&psyy)[V],
+                                       const T (&pvx)[V], const T (&psxy)[V], const Sweep<T>& cy) {
+    const T eps = tvd_eps<T>();
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      T d[4];
+      face_differences(f[VY][v] - pvy[v], f[SYY][v] - psyy[v], f[VX][v] - pvx[v],
+                       f[SXY][v] - psxy[v], cy, d[0], d[1], d[2], d[3]);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const T kc = q ? cy.kc2 : cy.kc1;
+        dfw[q][v] = d[2 * q];
+        const T dd = d[2 * q + 1];
+        const T q1 = eps - dd;
+        const T ps = psi(ratio(q1, q2[q][v]), kc);
+        bo[q][v] = fma(-ps, d2[q][v], c2[q][v]);
+        c2[q][v] = fma(ps, d2[q][v], dd);
+        d2[q][v] = dd;
+        q2[q][v] = q1;
+      }
+    }
+  }
+
+  __device__ __forceinline__ void apply(T (&gf)[NF][V], const Sweep<T>& cy) const {
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+      apply_increment<1>(gf[VX][v], gf[VY][v], gf[SXX][v], gf[SXY][v], gf[SYY][v], a2[0][v],
+                         bo[0][v], a2[1][v], bo[1][v], cy);
+  }
+
+  __device__ __forceinline__ void right(const Sweep<T>& cy) {
+    const T eps = tvd_eps<T>();
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const T kc = q ? cy.kc2 : cy.kc1;
+        const T dd = dfw[q][v];
+        const T p1 = dd + eps;
+        const T ps = psi(ratio(p2[q][v], p1), kc);
+        a2[q][v] = fma(-ps, dd, t2[q][v]);
+        t2[q][v] = fma(ps, dd, -dd);
+        p2[q][v] = p1;
+      }
+    }
+  }
+};
+
+// FP32: the same pipeline on pairs of columns with packed f32x2 arithmetic (the columns
+// are independent in the y-sweep).  Signs are arranged so that no negation is needed:
+// the right-moving state keeps -t and -A.  Reciprocals and the limiter's min/max/sat stay
+// per element.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 superbee2(float2 r) {
+  return f2(fmaxf(__saturatef(r.x + r.x), fminf(2.0f, r.x)),
+            fmaxf(__saturatef(r.y + r.y), fminf(2.0f, r.y)));
+}
+__device__ __forceinline__ float2 ratio2(float2 a, float2 b) {
+  float x, y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(x) : "f"(b.x));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b.y));
+  return mul2(a, f2(x, y));
+}
+
+template <int V>
+struct YPipe<float, V> {
+  static_assert(V % 2 == 0, "pairs of columns");
+  static constexpr int P = V / 2;
+  float2 p2[2][P], nt2[2][P], na2[2][P], q2[2][P], d2[2][P], c2[2][P];
+  float2 dfw[2][P], bo[2][P];
+
+  __device__ __forceinline__ void init() {
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) p2[q][i] = nt2[q][i] = na2[q][i] = q2[q][i] = d2[q][i] = c2[q][i] = f2(0.f, 0.f);
+  }
+
+  __device__ __forceinline__ void left(const float (&f)[NF][V], const float (&pvy)[V],
+                                       const float (&psyy)[V], const float (&pvx)[V],
+                                       const float (&psxy)[V], const Sweep<float>& cy) {
+    const float2 m1 = f2(-1.f, -1.f), eps = f2(1e-6f, 1e-6f);
+    const float2 nir1 = f2(-cy.irhoc1, -cy.irhoc1), ir1 = f2(cy.irhoc1, cy.irhoc1);
+    const float2 nir2 = f2(-cy.irhoc2, -cy.irhoc2), ir2 = f2(cy.irhoc2, cy.irhoc2);
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      const int a = 2 * i, b = 2 * i + 1;
+      const float2 dvn = fma2(f2(pvy[a], pvy[b]), m1, f2(f[VY][a], f[VY][b]));
+      const float2 dsn = fma2(f2(psyy[a], psyy[b]), m1, f2(f[SYY][a], f[SYY][b]));
+      const float2 dvt = fma2(f2(pvx[a], pvx[b]), m1, f2(f[VX][a], f[VX][b]));
+      const float2 dsx = fma2(f2(psxy[a], psxy[b]), m1, f2(f[SXY][a], f[SXY][b]));
+      const float2 d[4] = {fma2(dsn, nir1, dvn), fma2(dsn, ir1, dvn), fma2(dsx, nir2, dvt),
+                           fma2(dsx, ir2, dvt)};
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const float k = q ? cy.kc2 : cy.kc1;
+        dfw[q][i] = d[2 * q];
+        const float2 dd = d[2 * q + 1];
+        const float2 q1 = fma2(dd, m1, eps);  // eps - D
+        const float2 phi = superbee2(ratio2(q1, q2[q][i]));
+        const float2 ps = mul2(f2(k, k), phi), nps = mul2(f2(-k, -k), phi);
+        bo[q][i] = fma2(nps, d2[q][i], c2[q][i]);  // c - psi' D_{m-2}
+        c2[q][i] = fma2(ps, d2[q][i], dd);         // D + psi' D_{m-2}
+        d2[q][i] = dd;
+        q2[q][i] = q1;
+      }
+    }
+  }
+
+  __device__ __forceinline__ void apply(float (&gf)[NF][V], const Sweep<float>& cy) const {
+    const float2 m1 = f2(-1.f, -1.f);
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      const int a = 2 * i, b = 2 * i + 1;
+      const float2 s1 = fma2(na2[0][i], m1, bo[0][i]);  // A1 + B2
+      const float2 p1 = add2(bo[0][i], na2[0][i]);     // B2 - A1
+      const float2 s3 = fma2(na2[1][i], m1, bo[1][i]);  // A3 + B4
+      const float2 p3 = add2(bo[1][i], na2[1][i]);     // B4 - A3
+      const float2 vy = fma2(f2(cy.hk1, cy.hk1), s1, f2(gf[VY][a], gf[VY][b]));
+      const float2 vx = fma2(f2(cy.hk2, cy.hk2), s3, f2(gf[VX][a], gf[VX][b]));
+      const float2 syy = fma2(f2(cy.hk1rc1, cy.hk1rc1), p1, f2(gf[SYY][a], gf[SYY][b]));
+      const float2 sxx = fma2(f2(cy.hk1rc3, cy.hk1rc3), p1, f2(gf[SXX][a], gf[SXX][b]));
+      const float2 sxy = fma2(f2(cy.hk2rc2, cy.hk2rc2), p3, f2(gf[SXY][a], gf[SXY][b]));
+      gf[VY][a] = vy.x; gf[VY][b] = vy.y;
+      gf[VX][a] = vx.x; gf[VX][b] = vx.y;
+      gf[SYY][a] = syy.x; gf[SYY][b] = syy.y;
+      gf[SXX][a] = sxx.x; gf[SXX][b] = sxx.y;
+      gf[SXY][a] = sxy.x; gf[SXY][b] = sxy.y;
+    }
+  }
+
+  __device__ __forceinline__ void right(const Sweep<float>& cy) {
+    const float2 eps = f2(1e-6f, 1e-6f);
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const float k = q ? cy.kc2 : cy.kc1;
+        const float2 dd = dfw[q][i];
+        const float2 p1 = add2(dd, eps);
+        const float2 phi = superbee2(ratio2(p2[q][i], p1));
+        const float2 ps = mul2(f2(k, k), phi), nps = mul2(f2(-k, -k), phi);
+        na2[q][i] = fma2(ps, dd, nt2[q][i]);  // -(t_{m-2} - psi D)
+        nt2[q][i] = fma2(nps, dd, dd);        // -(psi - 1) D
+        p2[q][i] = p1;
+      }
+    }
+  }
+};
+
 // Advances one tile -- strip `strip` (32*V columns, halo lanes included), rows [y0, y1) --
-// by one step from g.src to g.dst.  `ring` = this warp's 3*NF*32*V elements of shared
-// memory.  Called by all 32 lanes of a warp.
-template <typename T, int V, int UNROLL, bool COHERENT, bool TAP>
+// by one step from g.src to g.dst.  `smem_warp` = this warp's warp_smem_elems() elements of
+// shared memory; every lane touches only its own V columns of it.  Called by all 32 lanes.
+template <typename T, int V, int NPF, bool COHERENT, bool TAP>
 __device__ __forceinline__ void march_tile(const GridRef<T>& g, const StepConsts<T>& c, int strip,
-                                           int y0, int y1, T* ring_warp, const RowTap<T>& tap) {
+                                           int y0, int y1, T* smem_warp, const RowTap<T>& tap) {
   using VT = typename Vec<T, V>::type;
+  static_assert(!COHERENT || V * sizeof(T) == 16, "coherent loads need 16-byte (L2-only) copies");
+  static_assert(NPF >= 2, "the input ring needs at least the current and the next row");
   constexpr int H = halo_lanes(V);
   constexpr int kIn = 32 * V;
   constexpr int kOut = strip_cols(V);
+  constexpr int kRow = NF * kIn;  // elements of one ring slot
   const int lane = threadIdx.x & 31;
-  T* ring = ring_warp + lane * V;
+  T* in_ring = smem_warp + lane * V;  // NPF slots of raw rows
+  T* xs_ring = in_ring + NPF * kRow;  // 3 slots of x-swept rows
   const int xs = strip * kOut - H * V;
   const int col0 = xs + lane * V;
   const bool interior = xs >= 0 && xs + kIn <= g.nx;
   const bool writer = lane >= H && lane < 32 - H && col0 < g.nx;
-  const T eps = tvd_eps<T>();
   const Sweep<T>& cy = c.y;
 
-  // y-pipeline state per column (face j lies between rows j and j+1): the fields of row
-  // m-1 that enter the y-invariants (vy, syy, vx, sxy); for w1/w3: P_{m-2}, t_{m-2} and
-  // A_{m-1} (written out one row later); for w2/w4: Q_{m-2}, D_{m-2}, c_{m-2}.
-  T pf[4][V], p2[2][V], t2[2][V], a2[2][V], q2[2][V], d2[2][V], c2[2][V];
+  // y-pipeline; the fields of row m-1 that enter the y-differences are read back from the
+  // x-swept ring
+  YPipe<T, V> yp;
+  yp.init();
+  // the slot read as "row y0-3" by the first row: zero, so no stale shared memory enters
 #pragma unroll
-  for (int v = 0; v < V; ++v) {
-#pragma unroll
-    for (int k = 0; k < 4; ++k) pf[k][v] = T(0);
-#pragma unroll
-    for (int q = 0; q < 2; ++q) p2[q][v] = t2[q][v] = a2[q][v] = q2[q][v] = d2[q][v] = c2[q][v] = T(0);
-  }
+  for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(xs_ring + 2 * kRow + k * kIn) = VT{};
 
-  T nxt[NF][V];
-  load_row<T, V, COHERENT>(nxt, g, source_row(y0 - 2, g.ny, g.far_rot), col0, interior);
-  int slot = 0;  // ring slot of row m; row m-2 sits in (slot + 1) % 3
-#pragma unroll UNROLL
+#pragma unroll
+  for (int j = 0; j < NPF - 1; ++j)
+    fetch_row<T, V, COHERENT>(in_ring + j * kRow, g, source_row(y0 - 2 + j, g.ny, g.far_rot), col0,
+                              interior);
+  int islot = 0;  // input slot of row m
+  int xslot = 0;  // x-swept slot of row m; row m-1 in (xslot + 2) % 3, row m-2 in (xslot + 1) % 3
   for (int m = y0 - 2; m < y1 + 2; ++m) {
+    {
+      const int mm = m + NPF - 1;
+      const int ns = islot + NPF - 1 >= NPF ? islot - 1 : islot + NPF - 1;
+      if (mm < y1 + 2)
+        fetch_row<T, V, COHERENT>(in_ring + ns * kRow, g, source_row(mm, g.ny, g.far_rot), col0,
+                                  interior);
+      else
+        cp_async_commit();  // keep one group per row
+    }
+    cp_async_wait<NPF - 1>();  // row m has landed
     T f[NF][V];
 #pragma unroll
     for (int k = 0; k < NF; ++k)
-#pragma unroll
-      for (int v = 0; v < V; ++v) f[k][v] = nxt[k][v];
-    if (m + 1 < y1 + 2)
-      load_row<T, V, COHERENT>(nxt, g, source_row(m + 1, g.ny, g.far_rot), col0, interior);
+      unpack(*reinterpret_cast<const VT*>(in_ring + islot * kRow + k * kIn), f[k]);
 
     sweep_x_lane<T, V>(f, c.x);
 
-    T* rs = ring + slot * (NF * kIn);
+    T* rs = xs_ring + xslot * kRow;
 #pragma unroll
     for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(rs + k * kIn) = pack(f[k]);
+    // rows m and m-1 as the y-pipeline reads them (16-byte loads land in aligned register
+    // groups, which the packed FP32 pipeline consumes without moves)
+    const T* rp = xs_ring + (xslot == 0 ? 2 : xslot - 1) * kRow;  // row m-1
+    T cur[NF][V], pvy[V], psyy[V], pvx[V], psxy[V];
+    unpack(*reinterpret_cast<const VT*>(rs + VY * kIn), cur[VY]);
+    unpack(*reinterpret_cast<const VT*>(rs + SYY * kIn), cur[SYY]);
+    unpack(*reinterpret_cast<const VT*>(rs + VX * kIn), cur[VX]);
+    unpack(*reinterpret_cast<const VT*>(rs + SXY * kIn), cur[SXY]);
+    unpack(*reinterpret_cast<const VT*>(rp + VY * kIn), pvy);
+    unpack(*reinterpret_cast<const VT*>(rp + SYY * kIn), psyy);
+    unpack(*reinterpret_cast<const VT*>(rp + VX * kIn), pvx);
+    unpack(*reinterpret_cast<const VT*>(rp + SXY * kIn), psxy);
 
-    T a_out[2][V], b_out[2][V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      // D_{m-1} of the four invariants from the field differences of rows m-1 and m
-      T d[4];
-      face_differences(f[VY][v] - pf[0][v], f[SYY][v] - pf[1][v], f[VX][v] - pf[2][v],
-                       f[SXY][v] - pf[3][v], cy, d[0], d[1], d[2], d[3]);
-      pf[0][v] = f[VY][v];
-      pf[1][v] = f[SYY][v];
-      pf[2][v] = f[VX][v];
-      pf[3][v] = f[SXY][v];
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const T kc = q ? cy.kc2 : cy.kc1;
-        {  // right-moving: psi_{m-1}, A_{m-1} = t_{m-2} - psi_{m-1} D_{m-1}, t_{m-1}
-          const T dd = d[2 * q];
-          const T p1 = dd + eps;
-          const T ps = psi(ratio(p2[q][v], p1), kc);
-          a_out[q][v] = a2[q][v];
-          a2[q][v] = fma(-ps, dd, t2[q][v]);
-          t2[q][v] = fma(ps, dd, -dd);
-          p2[q][v] = p1;
-        }
-        {  // left-moving: psi'_{m-1}, B_{m-2} = c_{m-2} - psi'_{m-1} D_{m-2}, c_{m-1}
-          const T dd = d[2 * q + 1];
-          const T q1 = eps - dd;
-          const T ps = psi(ratio(q1, q2[q][v]), kc);
-          b_out[q][v] = fma(-ps, d2[q][v], c2[q][v]);
-          c2[q][v] = fma(ps, d2[q][v], dd);
-          d2[q][v] = dd;
-          q2[q][v] = q1;
-        }
-      }
-    }
+    // D_{m-1} of the four invariants; left-moving part first: B_{m-2}, c_{m-1}
+    yp.left(cur, pvy, psyy, pvx, psxy, cy);
 
-    if (m >= y0 + 2) {  // whole warp: halo lanes compute too, only the stores are predicated
+    if (m >= y0 + 2) {  // row m-2 is complete (whole warp computes; stores are predicated)
       const int row = m - 2;
-      const T* rg = ring + (slot == 2 ? 0 : slot + 1) * (NF * kIn);
+      const T* rg = xs_ring + (xslot == 2 ? 0 : xslot + 1) * kRow;
       T gf[NF][V];
 #pragma unroll
       for (int k = 0; k < NF; ++k) unpack(*reinterpret_cast<const VT*>(rg + k * kIn), gf[k]);
-#pragma unroll
-      for (int v = 0; v < V; ++v)
-        apply_increment<1>(gf[VX][v], gf[VY][v], gf[SXX][v], gf[SXY][v], gf[SYY][v], a_out[0][v],
-                           b_out[0][v], a_out[1][v], b_out[1][v], cy);
+      yp.apply(gf, cy);
       if (writer) {
         T* out = g.dst + (long long)row * g.pitch + col0;
 #pragma unroll
@@ -262,7 +462,11 @@ __device__ __forceinline__ void march_tile(const GridRef<T>& g, const StepConsts
         }
       }
     }
-    slot = slot == 2 ? 0 : slot + 1;
+
+    // right-moving part: psi_{m-1}, A_{m-1} = t_{m-2} - psi_{m-1} D_{m-1}, t_{m-1}
+    yp.right(cy);
+    islot = islot + 1 == NPF ? 0 : islot + 1;
+    xslot = xslot == 2 ? 0 : xslot + 1;
   }
 }
 

@@ -5,8 +5,9 @@
 // The grid is cut into vertical strips (32 lanes x V columns, one warp each, the
 // outer lanes supplying the x-halo) and each strip into segments of seg_len rows;
 // every warp marches one strip segment (march.cuh).  Warps are independent, so a
-// block is just kWarps of them sharing the launch.
-#include "march.cuh"
+// block is just kWarps of them sharing the launch.  Variants of temporal-block depth 2
+// advance each tile by two steps per launch (march2.cuh).
+#include "march2.cuh"
 
 namespace le2d {
 
@@ -21,45 +22,72 @@ struct FusedParams {
 
 constexpr int kWarps = 4;  // warps per block
 
-template <typename T, int V, int MINB, int UNROLL>
+template <typename T, int V, int NPF, int D>
+__host__ __device__ constexpr int warp_elems() {
+  return D == 2 ? march::warp_smem_elems2<T, V, NPF>() : march::warp_smem_elems<T, V, NPF>();
+}
+
+template <typename T, int V, int MINB, int NPF, int D>
 __global__ void __launch_bounds__(kWarps * 32, MINB) fused_step_kernel(const FusedParams<T> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int wib = threadIdx.x >> 5;
   const int task = blockIdx.x * kWarps + wib;
   if (task >= p.ntasks) return;  // whole warp leaves together
-  T* ring = reinterpret_cast<T*>(smem_raw) + wib * (3 * NF * 32 * V);
+  T* smem = reinterpret_cast<T*>(smem_raw) + wib * warp_elems<T, V, NPF, D>();
   const int strip = task % p.nstrips;
   const int seg = task / p.nstrips;
   const int y0 = seg * p.seg_len;
   const int y1 = min(y0 + p.seg_len, p.g.ny);
-  march::march_tile<T, V, UNROLL, false, false>(p.g, p.c, strip, y0, y1, ring,
-                                                 march::RowTap<T>{nullptr, -1});
+  if constexpr (D == 2)
+    march::march_tile2<T, V, NPF, false>(p.g, p.c, strip, y0, y1, smem);
+  else
+    march::march_tile<T, V, NPF, false, false>(p.g, p.c, strip, y0, y1, smem,
+                                                march::RowTap<T>{nullptr, -1});
 }
 
 // Compiled variants: columns per lane V (one 16- or 8-byte access per field), the
-// minimum resident blocks per SM handed to the register allocator, and the unroll of
-// the row loop (2 lets the loop-carried y-pipeline state alternate registers).
+// minimum resident blocks per SM handed to the register allocator, the depth of the
+// shared-memory input ring (NPF - 1 rows are in flight ahead of the row being swept) and
+// the temporal-block depth D (steps per launch).
 template <typename T, int VAR>
 struct VariantCfg;
-template <> struct VariantCfg<float, 0> { static constexpr int V = 4, MINB = 3, UNROLL = 1; };
-template <> struct VariantCfg<float, 1> { static constexpr int V = 4, MINB = 1, UNROLL = 2; };
-template <> struct VariantCfg<float, 2> { static constexpr int V = 2, MINB = 4, UNROLL = 1; };
-template <> struct VariantCfg<float, 3> { static constexpr int V = 2, MINB = 4, UNROLL = 2; };
-template <> struct VariantCfg<float, 4> { static constexpr int V = 4, MINB = 3, UNROLL = 2; };
-template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 2, UNROLL = 1; };
-template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 3, UNROLL = 1; };
-template <> struct VariantCfg<double, 2> { static constexpr int V = 1, MINB = 4, UNROLL = 1; };
-template <> struct VariantCfg<double, 3> { static constexpr int V = 1, MINB = 4, UNROLL = 2; };
-template <> struct VariantCfg<double, 4> { static constexpr int V = 1, MINB = 3, UNROLL = 2; };
-constexpr int kVariants = 5;
+template <> struct VariantCfg<float, 0> { static constexpr int V = 4, MINB = 3, NPF = 2, D = 1; };
+template <> struct VariantCfg<float, 1> { static constexpr int V = 4, MINB = 3, NPF = 3, D = 1; };
+template <> struct VariantCfg<float, 2> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 1; };
+template <> struct VariantCfg<float, 3> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 1; };
+template <> struct VariantCfg<float, 4> { static constexpr int V = 2, MINB = 4, NPF = 3, D = 1; };
+template <> struct VariantCfg<float, 5> { static constexpr int V = 4, MINB = 2, NPF = 2, D = 2; };
+template <> struct VariantCfg<float, 6> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 2; };
+template <> struct VariantCfg<float, 7> { static constexpr int V = 2, MINB = 3, NPF = 3, D = 2; };
+template <> struct VariantCfg<float, 8> { static constexpr int V = 2, MINB = 5, NPF = 2, D = 2; };
+template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 1; };
+template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 1; };
+template <> struct VariantCfg<double, 2> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 1; };
+template <> struct VariantCfg<double, 3> { static constexpr int V = 1, MINB = 4, NPF = 3, D = 1; };
+template <> struct VariantCfg<double, 4> { static constexpr int V = 1, MINB = 5, NPF = 2, D = 1; };
+template <> struct VariantCfg<double, 5> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 2; };
+template <> struct VariantCfg<double, 6> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 2; };
+template <> struct VariantCfg<double, 7> { static constexpr int V = 1, MINB = 3, NPF = 3, D = 2; };
+template <> struct VariantCfg<double, 8> { static constexpr int V = 1, MINB = 5, NPF = 2, D = 2; };
+constexpr int kVariants = 9;
 
 template <typename T, int VAR>
 struct VariantKernel {
   using C = VariantCfg<T, VAR>;
-  static void* fn() { return (void*)fused_step_kernel<T, C::V, C::MINB, C::UNROLL>; }
-  static size_t smem() { return (size_t)kWarps * 3 * NF * 32 * C::V * sizeof(T); }
+  static void* fn() { return (void*)fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D>; }
+  static size_t smem() {
+    return (size_t)kWarps * warp_elems<T, C::V, C::NPF, C::D>() * sizeof(T);
+  }
+  // dynamic shared memory above 48 KB must be opted into once per kernel
+  static void prepare() {
+    static bool done = false;
+    if (!done) {
+      cudaFuncSetAttribute(fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+      done = true;
+    }
+  }
   static void launch(const FusedPlan& pl, const FusedParams<T>& p, cudaStream_t s) {
-    fused_step_kernel<T, C::V, C::MINB, C::UNROLL><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
+    fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
   }
 };
 
@@ -70,6 +98,10 @@ R with_variant(int var, A&&... a) {
     case 2: return Op<T, 2>::run(a...);
     case 3: return Op<T, 3>::run(a...);
     case 4: return Op<T, 4>::run(a...);
+    case 5: return Op<T, 5>::run(a...);
+    case 6: return Op<T, 6>::run(a...);
+    case 7: return Op<T, 7>::run(a...);
+    case 8: return Op<T, 8>::run(a...);
     default: return Op<T, 0>::run(a...);
   }
 }
@@ -79,9 +111,14 @@ struct LanesOp {
   static int run() { return VariantCfg<T, VAR>::V; }
 };
 template <typename T, int VAR>
+struct DepthOp {
+  static int run() { return VariantCfg<T, VAR>::D; }
+};
+template <typename T, int VAR>
 struct ResidentOp {
   static int run(int device) {
     int sms = 0, per_sm = 0;
+    VariantKernel<T, VAR>::prepare();
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, VariantKernel<T, VAR>::fn(), kWarps * 32,
                                                       VariantKernel<T, VAR>::smem()) != cudaSuccess)
@@ -91,7 +128,10 @@ struct ResidentOp {
 };
 template <typename T, int VAR>
 struct SmemOp {
-  static size_t run() { return VariantKernel<T, VAR>::smem(); }
+  static size_t run() {
+    VariantKernel<T, VAR>::prepare();
+    return VariantKernel<T, VAR>::smem();
+  }
 };
 template <typename T, int VAR>
 struct LaunchOp {
@@ -110,21 +150,34 @@ template <typename T>
 int fused_variant_lanes(int variant) { return with_variant<T, LanesOp, int>(variant); }
 
 template <typename T>
+int fused_variant_depth(int variant) { return with_variant<T, DepthOp, int>(variant); }
+
+template <typename T>
 int fused_resident_warps(int device, int variant) {
   return with_variant<T, ResidentOp, int>(variant, device);
 }
+
+// Segments are sized so the launch runs several waves of warps (kWaves): blocks are
+// dispatched in task order, so the warps resident at any moment cover one band of
+// neighbouring rows -- DRAM pages shared by adjacent strips, halo rows shared in L2 --
+// rather than rows a long segment apart.  Measured on the 8192^2 FP32 case: 32-row
+// segments (8 waves) run at 1.33e11 node-updates/s, single-wave 241-row segments at 1.0e11.
+// A two-step tile recomputes 8 halo rows of step A and 4 of step B, so its segments are
+// at least twice min_seg (at 4096^2: 32-row segments 1.17e11, 16-row 1.09e11).
+constexpr int kWaves = 8;
 
 template <typename T>
 FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_seg) {
   FusedPlan pl;
   pl.variant = variant < 0 || variant >= kVariants ? 0 : variant;
   pl.lanes = fused_variant_lanes<T>(pl.variant);
-  const int out = strip_cols(pl.lanes);
+  pl.depth = fused_variant_depth<T>(pl.variant);
+  const int out = pl.depth == 2 ? march::strip_cols2(pl.lanes) : strip_cols(pl.lanes);
   pl.nstrips = (nx + out - 1) / out;
-  int target = resident_warps > 0 ? resident_warps / pl.nstrips : 1;
+  int target = resident_warps > 0 ? kWaves * resident_warps / pl.nstrips : 1;
   if (target < 1) target = 1;
   int seg = (ny + target - 1) / target;
-  if (seg < min_seg) seg = min_seg;
+  if (seg < min_seg * pl.depth) seg = min_seg * pl.depth;
   if (seg > ny) seg = ny;
   pl.seg_len = seg;
   pl.nsegs = (ny + seg - 1) / seg;
@@ -139,6 +192,7 @@ template <typename T>
 cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pitch,
                               long long plane, const StepConsts<T>& c, int far_rot,
                               const FusedPlan& plan, cudaStream_t s) {
+  if (plan.depth == 2 && far_rot) return cudaErrorInvalidValue;  // two steps assume clamped ends
   FusedParams<T> p;
   p.g = march::GridRef<T>{src, dst, nx, ny, pitch, plane, far_rot};
   p.nstrips = plan.nstrips;
@@ -152,6 +206,7 @@ cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pi
 #define LE2D_INST(T)                                                                            \
   template int fused_variant_count<T>();                                                        \
   template int fused_variant_lanes<T>(int);                                                     \
+  template int fused_variant_depth<T>(int);                                                     \
   template int fused_resident_warps<T>(int, int);                                               \
   template FusedPlan plan_fused<T>(int, int, int, int, int);                                    \
   template cudaError_t launch_fused_step<T>(const T*, T*, int, int, long long, long long,       \

@@ -155,15 +155,34 @@ def test_step_n_equals_single_steps(libs, prec):
     assert a.tobytes() == b.tobytes()
 
 
+def variants(lib):
+    """Compiled fused-kernel variants with their temporal-block depth: {variant: depth}."""
+    c = dict(nx=8, ny=8, hx=1.0, hy=1.0, c1=2.0, c2=1.0, rho=1.0, dt=0.25, stype=ST_AOS)
+    t = make_task(lib, c)
+    out = {}
+    try:
+        v = 0
+        while lib.set_variant(t, v, 0) == 0:
+            out[v] = lib.get_plan(t)["depth"]
+            v += 1
+    finally:
+        lib.le_free_task(t)
+    return out
+
+
 @pytest.mark.parametrize("prec", ["f", "d"])
 def test_variants_and_segments_bitwise_equal(libs, prec):
     """Every compiled variant and row-segment length computes the same per-node operations,
-    so results are bitwise equal; also matches the oracle (AoS and SoA far end)."""
+    so results are bitwise equal; also matches the oracle (AoS and SoA far end).  Variants
+    of temporal-block depth 2 run two steps per launch (AoS; the SoA far end takes single
+    steps), with the odd last step of 41 as a single step."""
     lib = libs[prec]
+    vs = variants(lib)
+    assert sorted(set(vs.values())) == [1, 2]
     for stype in (ST_AOS, ST_SOA):
-        p, g0, steps = _medium(prec, stype, 263, 171, 40)
+        p, g0, steps = _medium(prec, stype, 263, 171, 41)
         outs = []
-        for var in range(5):
+        for var in sorted(vs):
             for seg in (0, 7, 33, 171):
                 t = make_task(lib, p)
                 try:
@@ -182,6 +201,45 @@ def test_variants_and_segments_bitwise_equal(libs, prec):
         gd = g0.astype(np.float64)
         Oracle("d").run(gd, p["nx"], p["ny"], p["dt"], p["hx"], p["hy"], p["c1"], p["c2"], p["rho"], stype, steps)
         check(prec, outs[0][1], want, gd, p["nx"], p["ny"], stype, f"variants/{prec}/{stype}")
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_temporal_blocking_edges(libs, prec):
+    """Two steps per launch on grids and segments that put the clamped ends everywhere a
+    tile can meet them: widths around the strip width (one strip, two strips, a last strip
+    of one column), heights below and around the segment length, segments of 1 and 3 rows.
+    Bitwise equal to single steps, and to the oracle within tolerance."""
+    lib = libs[prec]
+    vs = variants(lib)
+    two = [v for v, d in vs.items() if d == 2]
+    one = [v for v, d in vs.items() if d == 1][0]
+    rng = np.random.default_rng(11)
+    for nx, ny in ((3, 3), (5, 4), (9, 7), (57, 3), (111, 20), (112, 33), (113, 17), (225, 9), (130, 64)):
+        c = dict(nx=nx, ny=ny, hx=1.0, hy=0.9, c1=2.0, c2=1.1, rho=1.3, dt=0.2, stype=ST_AOS)
+        o = Oracle(prec)
+        g0 = rng.uniform(-1, 1, size=5 * nx * ny).astype(o.dtype)
+        steps = 9
+        want = g0.copy()
+        o.run(want, nx, ny, c["dt"], c["hx"], c["hy"], c["c1"], c["c2"], c["rho"], ST_AOS, steps)
+        gd = g0.astype(np.float64)
+        Oracle("d").run(gd, nx, ny, c["dt"], c["hx"], c["hy"], c["c1"], c["c2"], c["rho"], ST_AOS, steps)
+        ref = None
+        for var, seg in [(one, 0)] + [(v, s) for v in two for s in (0, 1, 3, 5, 16)]:
+            t = make_task(lib, c)
+            try:
+                assert lib.set_variant(t, var, seg) == 0
+                assert lib.upload(t, g0.copy()) == 0
+                assert lib.step_n(t, steps) == 0
+                got = np.zeros_like(g0)
+                assert lib.download(t, got) == 0
+                assert lib.last_error(t) == 0
+            finally:
+                lib.le_free_task(t)
+            if ref is None:
+                ref = got
+                check(prec, got, want, gd, nx, ny, ST_AOS, f"edges/{prec}/{nx}x{ny}")
+            else:
+                assert got.tobytes() == ref.tobytes(), (nx, ny, var, seg)
 
 
 @pytest.mark.parametrize("prec", ["f", "d"])
