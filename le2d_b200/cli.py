@@ -2,12 +2,15 @@
 
     python -m le2d_b200.cli nx ny steps [--prec f|d] [--method fused|split]
                             [--workload plain|disks] [--save out.vtk]
+                            [--variant K --seg ROWS] [--per-call]
 
 Like simple/main.c:18-80: init material and task, set the initial condition, run
 `steps` calls of le_step, print "nx ny steps seconds" (simple/main.c:68) and
 optionally save the VTK.  The default initial condition is the reference driver's
 (c1=2, c2=1, rho=1.5, dt=0.3, one disk r=10 at the centre, s=1); --workload disks
 uses the seeded 8-disk material of the 8192x8192 workload scaled to the grid.
+--variant / --seg pick a compiled fused-kernel variant and row-segment length
+(le2d_set_variant) and print the plan, e.g. to profile one kernel variant.
 """
 from __future__ import annotations
 
@@ -28,6 +31,8 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", default="plain", choices=["plain", "disks"])
     ap.add_argument("--save", default=None)
     ap.add_argument("--per-call", action="store_true", help="one le_step call per step (default: le2d_step_n)")
+    ap.add_argument("--variant", type=int, default=None, help="fused-kernel variant (le2d_set_variant)")
+    ap.add_argument("--seg", type=int, default=0, help="row-segment length with --variant (0 = planner's)")
     a = ap.parse_args(argv)
     lib = capi.Lib(a.prec)
     if a.workload == "plain":
@@ -42,6 +47,11 @@ def main(argv=None) -> int:
         return 1
     try:
         lib.set_method(t, capi.LE2D_METHOD_FUSED if a.method == "fused" else capi.LE2D_METHOD_SPLIT)
+        if a.variant is not None:
+            if lib.set_variant(t, a.variant, a.seg) != 0:
+                print(f"no fused-kernel variant {a.variant}", file=sys.stderr)
+                return 1
+            print("plan", lib.get_plan(t))
         for cx, cy, r, s in disks:
             lib.le_set_ball(t, (cx, cy), r, s)
         lib.wait(t)

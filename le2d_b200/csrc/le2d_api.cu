@@ -43,6 +43,8 @@ struct DevTask {
   T* buf[2] = {nullptr, nullptr};
   int cur = 0;
   double* d_diag = nullptr;
+  int* d_status = nullptr;    // set by a warp-pair launch whose wait gave up
+  bool pairs_queued = false;  // warp-pair launches since d_status was last read
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   bool pinned = false;     // task->grid from cudaHostAlloc
@@ -62,6 +64,9 @@ struct DevTask {
 };
 
 constexpr int kGraphSteps = 64;  // even, so a replay leaves the current buffer unchanged
+// Bound of every wait between the two warps of a warp-pair tile (they share a block, so a
+// wait that long means a fault in the kernel, not a slow partner).
+constexpr unsigned long long kPairWaitNs = 1000000000ull;
 
 std::mutex g_mu;
 std::unordered_map<const void*, DevTask*> g_tasks;
@@ -95,13 +100,13 @@ DevTask* lookup(const le_task* task) {
 long long row_pitch(int nx) { return le2d::row_pitch_elems(nx); }
 
 // Fused-kernel variant used for new tasks: LE2D_FUSED_VARIANT if set, else the fastest
-// measured on large grids (FP32: two steps per launch, 2 columns per lane, 16 warps per SM;
-// FP64: one step per launch, 2 columns per lane -- two-step FP64 tiles need twice the
-// registers and run at 8 warps per SM).
+// measured on large grids (FP32: two steps per launch on producer / consumer warp pairs,
+// 4 columns per lane, 16 warps per SM; FP64: one step per launch, 2 columns per lane --
+// the FP64 two-step variants measured slower).
 int default_variant() {
   static int v = -2;
   if (v == -2) {
-    const int dflt = sizeof(T) == 4 ? 7 : 0;
+    const int dflt = sizeof(T) == 4 ? 9 : 0;
     const char* e = getenv("LE2D_FUSED_VARIANT");
     v = e ? atoi(e) : dflt;
     if (v < 0 || v >= le2d::fused_variant_count<T>()) v = dflt;
@@ -116,7 +121,7 @@ void replan(DevTask* d, int variant, int seg_len) {
   const int resident = le2d::fused_resident_warps<T>(dev, variant);
   le2d::FusedPlan p = le2d::plan_fused<T>(d->nx, d->ny, variant, resident, kMinSeg);
   if (seg_len > 0) {  // explicit segment length (tuning)
-    const int wpb = p.threads / 32;
+    const int wpb = p.threads / 32 / p.warps_per_task;  // tiles per block
     p.seg_len = seg_len < d->ny ? seg_len : d->ny;
     p.nsegs = (d->ny + p.seg_len - 1) / p.seg_len;
     p.ntasks = p.nstrips * p.nsegs;
@@ -176,6 +181,8 @@ int tune_size(int nx, int ny, Tuned* best) {
   e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&d->ev[0]);
   if (e == cudaSuccess) e = cudaEventCreate(&d->ev[1]);
+  if (e == cudaSuccess) e = cudaMalloc(&d->d_status, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d->d_status, 0, sizeof(int), d->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d->mem, 0, sizeof(T) * 2 * 5 * (size_t)d->plane, d->stream);
   if (e == cudaSuccess)
     e = le2d::launch_set_ball<T>(d->buf[0], nx, ny, d->pitch, d->plane, 1, 1, nx / 2, ny / 2,
@@ -253,6 +260,18 @@ bool same_consts(const StepConsts<T>& a, const StepConsts<T>& b) {
   return memcmp(&a, &b, sizeof(a)) == 0;
 }
 
+// After the task's stream has drained: reports (once) a warp-pair launch whose wait gave up.
+int check_pairs(DevTask* d) {
+  if (!d->pairs_queued || !d->d_status) return LE2D_OK;
+  d->pairs_queued = false;
+  int h = 0;
+  cudaError_t e = cudaMemcpy(&h, d->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return record(d, LE2D_ECUDA, "status read", e);
+  if (h == 0) return LE2D_OK;
+  cudaMemset(d->d_status, 0, sizeof(int));
+  return record(d, LE2D_ETIMEOUT, "step: a warp of a two-step tile gave up waiting for its partner");
+}
+
 int upload_raw(DevTask* d, const T* host, int aos) {
   const size_t bytes = sizeof(T) * 5 * (size_t)d->nx * d->ny;
   T* stage = d->buf[d->cur ^ 1];
@@ -273,7 +292,7 @@ int download_raw(DevTask* d, T* host, int aos) {
   if (e != cudaSuccess) return record(d, LE2D_ECUDA, "download", e);
   e = cudaStreamSynchronize(d->stream);
   if (e != cudaSuccess) return record(d, LE2D_ECUDA, "download sync", e);
-  return LE2D_OK;
+  return check_pairs(d);
 }
 
 int ensure_device_current(DevTask* d, le_task* task) {
@@ -313,8 +332,9 @@ cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int meth
   }
   const bool two = d->plan.depth == 2 && max_steps >= 2 && !far_rot;
   const FusedPlan& pl = two ? d->plan : d->plan1;
+  if (pl.warps_per_task == 2) d->pairs_queued = true;
   cudaError_t e = le2d::launch_fused_step<T>(a, b, d->nx, d->ny, d->pitch, d->plane, c, far_rot,
-                                             pl, d->stream);
+                                             pl, d->d_status, kPairWaitNs, d->stream);
   *cur ^= 1;
   *done += pl.depth;
   return e;
@@ -381,6 +401,8 @@ int run_steps(le_task* task, int nsteps, bool soa_entry, float* ms) {
     if (e == cudaSuccess) e = cudaEventSynchronize(d->ev[1]);
     if (e == cudaSuccess) e = cudaEventElapsedTime(ms, d->ev[0], d->ev[1]);
     if (e != cudaSuccess) return record(d, LE2D_ECUDA, "step timing", e);
+    const int rc2 = check_pairs(d);
+    if (rc2) return rc2;
   }
   // FP64 simulated-time accumulator: one dt per step.
   for (int s = 0; s < nsteps; ++s) d->sim_time += (double)task->dt;
@@ -399,6 +421,7 @@ void release(DevTask* d) {
   }
   if (d->mem) cudaFree(d->mem);
   if (d->d_diag) cudaFree(d->d_diag);
+  if (d->d_status) cudaFree(d->d_status);
   delete d;
 }
 
@@ -520,6 +543,8 @@ void le_init_task(le_task* task, const real dt, const le_vec2 h, const le_materi
       if (e == cudaSuccess) e = cudaEventCreate(&d->ev[0]);
       if (e == cudaSuccess) e = cudaEventCreate(&d->ev[1]);
       if (e == cudaSuccess) e = cudaMalloc(&d->d_diag, 16 * sizeof(double));
+      if (e == cudaSuccess) e = cudaMalloc(&d->d_status, sizeof(int));
+      if (e == cudaSuccess) e = cudaMemsetAsync(d->d_status, 0, sizeof(int), d->stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(d->mem, 0, dbytes, d->stream);
       if (e != cudaSuccess) {
         record(d, LE2D_ECUDA, "le_init_task: device setup", e);
@@ -702,7 +727,7 @@ int le2d_wait(le_task* task) {
   if (!d) return LE2D_ENOTASK;
   if (!d->has_device) return LE2D_OK;
   cudaError_t e = cudaStreamSynchronize(d->stream);
-  return e == cudaSuccess ? LE2D_OK : record(d, LE2D_ECUDA, "wait", e);
+  return e == cudaSuccess ? check_pairs(d) : record(d, LE2D_ECUDA, "wait", e);
 }
 
 int le2d_set_method(le_task* task, int method) {
@@ -743,7 +768,8 @@ int le2d_autotune(int nx, int ny, int* out_plan, double* nu_per_s) {
     out_plan[2] = t.seg_len > 0 ? (t.seg_len < ny ? t.seg_len : ny) : p.seg_len;
     out_plan[3] = p.nstrips;
     out_plan[4] = p.nstrips * ((ny + out_plan[2] - 1) / out_plan[2]);
-    out_plan[5] = (out_plan[4] + p.threads / 32 - 1) / (p.threads / 32);
+    const int tpb = p.threads / 32 / p.warps_per_task;  // tiles per block
+    out_plan[5] = (out_plan[4] + tpb - 1) / tpb;
     out_plan[6] = p.depth;
   }
   return LE2D_OK;

@@ -18,7 +18,8 @@ __host__ __device__ constexpr int strip_cols(int lanes) { return (32 - 2 * halo_
 
 struct FusedPlan {
   int variant = 0, lanes = 0;
-  int depth = 1;  // temporal-block depth: steps per launch
+  int depth = 1;           // temporal-block depth: steps per launch
+  int warps_per_task = 1;  // 2: a producer / consumer warp pair per tile (march_pair.cuh)
   int nstrips = 0, seg_len = 0, nsegs = 0, ntasks = 0;
   int blocks = 0, threads = 0;
   size_t smem = 0;
@@ -40,11 +41,13 @@ template <typename T>
 int fused_resident_warps(int device, int variant);
 
 // One fused launch src -> dst: plan.depth time steps.  far_rot selects the le_step_soa
-// far-end rows (depth-1 plans only).
+// far-end rows (depth-1 plans only).  Warp-pair plans bound every wait between the warps
+// of a pair by wait_ns and set *status (a device int) if one gave up.
 template <typename T>
 cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pitch,
                               long long plane, const StepConsts<T>& c, int far_rot,
-                              const FusedPlan& plan, cudaStream_t s);
+                              const FusedPlan& plan, int* status, unsigned long long wait_ns,
+                              cudaStream_t s);
 
 // The plain scheme: one sweep (axis 0 = x, 1 = y) src -> dst, one thread per node, the
 // reference's tvd2 formula node by node (two divisions per invariant).

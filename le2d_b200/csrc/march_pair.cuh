@@ -1,0 +1,232 @@
+// Two time steps per launch on a warp pair.  The tile's first step (step A) and second
+// step (step B) run on two warps of one block: the producer warp reads the state, x-sweeps
+// and y-sweeps it (step A) and hands each finished row to the consumer warp through a
+// small shared-memory queue; the consumer x-sweeps and y-sweeps those rows (step B) and
+// writes the result.  Each warp holds one y-pipeline, so four columns per lane fit in
+// 128 registers and 16 warps per SM, where one warp holding both steps needs twice the
+// pipeline state (march2.cuh).
+//
+// Queue.  kHand slots of one row (5 fields x 32V columns), each with two mbarriers of
+// arrival count 32: `full` (every producer lane arrives after writing its columns) and
+// `empty` (every consumer lane arrives after reading its columns).  The u-th handoff
+// uses slot u % kHand, its (u / kHand)-th use: the consumer waits for phase u / kHand of
+// `full`, the producer (from the second use of a slot on) for phase u / kHand - 1 of
+// `empty`.  Each lane reads back exactly the columns the same lane of the other warp wrote.
+//
+// Every wait is bounded by `wait_ns` of global time; a warp that gives up sets *status
+// and leaves, so its partner gives up too and the launch ends with the status set.
+//
+// Halos and boundaries as in march2.cuh: step A is valid on [xs+2, xs+32V-2), step B on
+// [xs+4, xs+32V-4); the producer overwrites step A's values outside [0, nx) with the edge
+// column's and hands row 0 / ny-1 over once and the consumer feeds it to step B once for
+// every row of its stencil it stands for (the same count both warps compute).
+#pragma once
+
+#include "march2.cuh"
+
+namespace le2d {
+namespace march {
+
+constexpr int kHand = 2;  // queue slots between the warps of a pair
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_timer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits (all 32 lanes) for the completion of the phase of `bar` with parity `parity`.
+// Returns false, warp-uniformly, if it has not completed within wait_ns or the partner
+// has already given up (*status != 0).
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity,
+                                          unsigned long long wait_ns, int* status) {
+  bool ok = mbar_test(bar, parity);
+  if (__all_sync(0xffffffffu, ok)) return true;
+  const unsigned long long t0 = global_timer_ns();
+  while (true) {
+    if (!ok) ok = mbar_test(bar, parity);
+    if (__all_sync(0xffffffffu, ok)) return true;
+    int bail = 0;
+    if ((threadIdx.x & 31) == 0)
+      bail = *reinterpret_cast<volatile int*>(status) != 0 || global_timer_ns() - t0 > wait_ns;
+    if (__shfl_sync(0xffffffffu, bail, 0)) {
+      if ((threadIdx.x & 31) == 0) atomicExch(status, 1);
+      return false;
+    }
+  }
+}
+
+// Shared memory of one pair: the producer's input ring (NPF rows) and step-A ring (3),
+// the queue (kHand), the consumer's step-B ring (3), each row NF x 32V elements; then
+// 2 * kHand mbarriers.
+template <typename T, int V, int NPF>
+__host__ __device__ constexpr int pair_smem_elems() {
+  return (NPF + 3 + kHand + 3) * NF * 32 * V;
+}
+template <typename T, int V, int NPF>
+__host__ __device__ constexpr int pair_smem_bytes() {
+  return pair_smem_elems<T, V, NPF>() * (int)sizeof(T) + 2 * kHand * 8;
+}
+
+// How many rows of step B's stencil step-A row ka stands for (tile rows [y0, y1)):
+// step B reads rows [y0-2, y1+2) clamped to [0, ny).
+__device__ __forceinline__ int row_uses(int ka, int y0, int y1, int ny) {
+  int reps = ka < 0 || ka >= ny ? 0 : 1;
+  if (ka == 0 && y0 < 2) reps += 2 - y0;
+  if (ka == ny - 1 && y1 + 2 > ny) reps += y1 + 2 - ny;
+  return reps;
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void pair_init(unsigned long long* bars) {
+  if ((threadIdx.x & 31) == 0)
+    for (int i = 0; i < 2 * kHand; ++i) mbar_init(bars + i, 32);
+}
+
+// Producer warp: step A of strip `strip`, rows [y0, y1) of the tile.
+template <typename T, int V, int NPF>
+__device__ __forceinline__ void pair_produce(const GridRef<T>& g, const StepConsts<T>& c, int strip,
+                                             int y0, int y1, T* smem_pair,
+                                             unsigned long long* bars,
+                                             unsigned long long wait_ns, int* status) {
+  using VT = typename Vec<T, V>::type;
+  static_assert(NPF >= 2, "the input ring needs at least the current and the next row");
+  constexpr int H2 = halo_lanes2(V);
+  constexpr int kIn = 32 * V;
+  constexpr int kOut = strip_cols2(V);
+  constexpr int kRow = NF * kIn;
+  const int lane = threadIdx.x & 31;
+  T* in_ring = smem_pair + lane * V;
+  T* a_ring = in_ring + NPF * kRow;
+  T* hand = a_ring + 3 * kRow;
+  unsigned long long* full = bars;
+  unsigned long long* empty = bars + kHand;
+  const int xs = strip * kOut - H2 * V;
+  const int col0 = xs + lane * V;
+  const bool interior = xs >= 0 && xs + kIn <= g.nx;
+
+  YPipe<T, V> ya;
+  ya.init();
+#pragma unroll
+  for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(a_ring + 2 * kRow + k * kIn) = VT{};
+#pragma unroll
+  for (int j = 0; j < NPF - 1; ++j)
+    fetch_row<T, V, false>(in_ring + j * kRow, g, source_row(y0 - 4 + j, g.ny, 0), col0, interior);
+  int islot = 0, aslot = 0;
+  unsigned u = 0;  // handoffs so far
+  for (int m = y0 - 4; m < y1 + 4; ++m) {
+    {
+      const int mm = m + NPF - 1;
+      const int ns = islot + NPF - 1 >= NPF ? islot - 1 : islot + NPF - 1;
+      if (mm < y1 + 4)
+        fetch_row<T, V, false>(in_ring + ns * kRow, g, source_row(mm, g.ny, 0), col0, interior);
+      else
+        cp_async_commit();
+    }
+    cp_async_wait<NPF - 1>();
+    T f[NF][V];
+#pragma unroll
+    for (int k = 0; k < NF; ++k)
+      unpack(*reinterpret_cast<const VT*>(in_ring + islot * kRow + k * kIn), f[k]);
+    sweep_x_lane<T, V>(f, c.x);
+    ring_left(ya, f, a_ring, aslot, c.y);
+    const int ka = m - 2;  // step-A row completed now
+    if (m >= y0 && row_uses(ka, y0, y1, g.ny) > 0) {
+      T ga[NF][V];
+      ring_output(ya, ga, a_ring, aslot, c.y);
+      if (!interior) clamp_columns<T, V>(ga, xs, col0, g.nx);
+      const int hs = (int)(u % kHand);
+      const unsigned use = u / kHand;
+      if (use > 0 && !mbar_wait(empty + hs, (use - 1) & 1, wait_ns, status)) break;
+      T* slot = hand + hs * kRow;
+#pragma unroll
+      for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(slot + k * kIn) = pack(ga[k]);
+      mbar_arrive(full + hs);
+      ++u;
+    }
+    ya.right(c.y);
+    islot = islot + 1 == NPF ? 0 : islot + 1;
+    aslot = aslot == 2 ? 0 : aslot + 1;
+  }
+  cp_async_wait<0>();  // nothing of this warp's in flight when it leaves (also after a break)
+}
+
+// Consumer warp: step B of the same tile, writing rows [y0, y1) to g.dst.
+template <typename T, int V, int NPF>
+__device__ __forceinline__ void pair_consume(const GridRef<T>& g, const StepConsts<T>& c, int strip,
+                                             int y0, int y1, T* smem_pair,
+                                             unsigned long long* bars,
+                                             unsigned long long wait_ns, int* status) {
+  using VT = typename Vec<T, V>::type;
+  constexpr int H2 = halo_lanes2(V);
+  constexpr int kIn = 32 * V;
+  constexpr int kOut = strip_cols2(V);
+  constexpr int kRow = NF * kIn;
+  const int lane = threadIdx.x & 31;
+  T* hand = smem_pair + lane * V + (NPF + 3) * kRow;
+  T* b_ring = hand + kHand * kRow;
+  unsigned long long* full = bars;
+  unsigned long long* empty = bars + kHand;
+  const int xs = strip * kOut - H2 * V;
+  const int col0 = xs + lane * V;
+  const bool writer = lane >= H2 && lane < 32 - H2 && col0 < g.nx;
+
+  YPipe<T, V> yb;
+  yb.init();
+#pragma unroll
+  for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(b_ring + 2 * kRow + k * kIn) = VT{};
+  int bslot = 0;
+  int bin = y0 - 2;  // step-B row index of the next row fed to step B
+  unsigned u = 0;
+  for (int ka = y0 - 2; ka < y1 + 2; ++ka) {
+    const int reps = row_uses(ka, y0, y1, g.ny);
+    if (reps == 0) continue;
+    const int hs = (int)(u % kHand);
+    if (!mbar_wait(full + hs, (u / kHand) & 1, wait_ns, status)) return;
+    const T* slot = hand + hs * kRow;
+    for (int r = 0; r < reps; ++r) {  // the slot is read once per use, released after the last
+      T fb[NF][V];
+#pragma unroll
+      for (int k = 0; k < NF; ++k) unpack(*reinterpret_cast<const VT*>(slot + k * kIn), fb[k]);
+      if (r == reps - 1) mbar_arrive(empty + hs);
+      sweep_x_lane<T, V>(fb, c.x);
+      ring_left(yb, fb, b_ring, bslot, c.y);
+      if (bin >= y0 + 2) {  // step-B row bin-2 is complete
+        T gb[NF][V];
+        ring_output(yb, gb, b_ring, bslot, c.y);
+        if (writer) {
+          T* out = g.dst + (long long)(bin - 2) * g.pitch + col0;
+#pragma unroll
+          for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(out + k * g.plane) = pack(gb[k]);
+        }
+      }
+      yb.right(c.y);
+      bslot = bslot == 2 ? 0 : bslot + 1;
+      ++bin;
+    }
+    ++u;
+  }
+}
+
+}  // namespace march
+}  // namespace le2d

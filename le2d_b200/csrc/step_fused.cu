@@ -6,8 +6,9 @@
 // outer lanes supplying the x-halo) and each strip into segments of seg_len rows;
 // every warp marches one strip segment (march.cuh).  Warps are independent, so a
 // block is just kWarps of them sharing the launch.  Variants of temporal-block depth 2
-// advance each tile by two steps per launch (march2.cuh).
-#include "march2.cuh"
+// advance each tile by two steps per launch, on one warp (march2.cuh) or on a producer /
+// consumer warp pair (march_pair.cuh).
+#include "march_pair.cuh"
 
 namespace le2d {
 
@@ -18,6 +19,8 @@ struct FusedParams {
   march::GridRef<T> g;
   int nstrips, seg_len, ntasks;
   StepConsts<T> c;
+  int* status;                 // warp pairs: set when a wait gave up
+  unsigned long long wait_ns;  // warp pairs: bound of every wait
 };
 
 constexpr int kWarps = 4;  // warps per block
@@ -45,38 +48,77 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) fused_step_kernel(const Fus
                                                 march::RowTap<T>{nullptr, -1});
 }
 
+// Two-step tiles on warp pairs: kWarps / 2 pairs per block, each with its own shared
+// memory and queue barriers.  The barriers are initialised before the block's barrier, so
+// both warps of a pair see them, and the pair leaves together (same tile).
+template <typename T, int V, int MINB, int NPF>
+__global__ void __launch_bounds__(kWarps * 32, MINB) fused_pair_kernel(const FusedParams<T> p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int kPairs = kWarps / 2;
+  const int wib = threadIdx.x >> 5;
+  const int pair = wib >> 1;
+  unsigned char* base = smem_raw + pair * march::pair_smem_bytes<T, V, NPF>();
+  unsigned long long* bars =
+      reinterpret_cast<unsigned long long*>(base + march::pair_smem_elems<T, V, NPF>() * sizeof(T));
+  if ((wib & 1) == 0) march::pair_init<T, V>(bars);
+  __syncthreads();
+  const int task = blockIdx.x * kPairs + pair;
+  if (task >= p.ntasks) return;  // both warps of the pair
+  const int strip = task % p.nstrips;
+  const int seg = task / p.nstrips;
+  const int y0 = seg * p.seg_len;
+  const int y1 = min(y0 + p.seg_len, p.g.ny);
+  T* smem = reinterpret_cast<T*>(base);
+  if ((wib & 1) == 0)
+    march::pair_produce<T, V, NPF>(p.g, p.c, strip, y0, y1, smem, bars, p.wait_ns, p.status);
+  else
+    march::pair_consume<T, V, NPF>(p.g, p.c, strip, y0, y1, smem, bars, p.wait_ns, p.status);
+}
+
 // Compiled variants: columns per lane V (one 16- or 8-byte access per field), the
 // minimum resident blocks per SM handed to the register allocator, the depth of the
-// shared-memory input ring (NPF - 1 rows are in flight ahead of the row being swept) and
-// the temporal-block depth D (steps per launch).
+// shared-memory input ring (NPF - 1 rows are in flight ahead of the row being swept),
+// the temporal-block depth D (steps per launch) and P = 1 for two-step tiles on warp pairs.
 template <typename T, int VAR>
 struct VariantCfg;
-template <> struct VariantCfg<float, 0> { static constexpr int V = 4, MINB = 3, NPF = 2, D = 1; };
-template <> struct VariantCfg<float, 1> { static constexpr int V = 4, MINB = 3, NPF = 3, D = 1; };
-template <> struct VariantCfg<float, 2> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 1; };
-template <> struct VariantCfg<float, 3> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 1; };
-template <> struct VariantCfg<float, 4> { static constexpr int V = 2, MINB = 4, NPF = 3, D = 1; };
-template <> struct VariantCfg<float, 5> { static constexpr int V = 4, MINB = 2, NPF = 2, D = 2; };
-template <> struct VariantCfg<float, 6> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 2; };
-template <> struct VariantCfg<float, 7> { static constexpr int V = 2, MINB = 3, NPF = 3, D = 2; };
-template <> struct VariantCfg<float, 8> { static constexpr int V = 2, MINB = 5, NPF = 2, D = 2; };
-template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 1; };
-template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 1; };
-template <> struct VariantCfg<double, 2> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 1; };
-template <> struct VariantCfg<double, 3> { static constexpr int V = 1, MINB = 4, NPF = 3, D = 1; };
-template <> struct VariantCfg<double, 4> { static constexpr int V = 1, MINB = 5, NPF = 2, D = 1; };
-template <> struct VariantCfg<double, 5> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 2; };
-template <> struct VariantCfg<double, 6> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 2; };
-template <> struct VariantCfg<double, 7> { static constexpr int V = 1, MINB = 3, NPF = 3, D = 2; };
-template <> struct VariantCfg<double, 8> { static constexpr int V = 1, MINB = 5, NPF = 2, D = 2; };
-constexpr int kVariants = 9;
+template <> struct VariantCfg<float, 0> { static constexpr int V = 4, MINB = 3, NPF = 2, D = 1, P = 0; };
+template <> struct VariantCfg<float, 1> { static constexpr int V = 4, MINB = 3, NPF = 3, D = 1, P = 0; };
+template <> struct VariantCfg<float, 2> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 1, P = 0; };
+template <> struct VariantCfg<float, 3> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 1, P = 0; };
+template <> struct VariantCfg<float, 4> { static constexpr int V = 2, MINB = 4, NPF = 3, D = 1, P = 0; };
+template <> struct VariantCfg<float, 5> { static constexpr int V = 4, MINB = 2, NPF = 2, D = 2, P = 0; };
+template <> struct VariantCfg<float, 6> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 2, P = 0; };
+template <> struct VariantCfg<float, 7> { static constexpr int V = 2, MINB = 3, NPF = 3, D = 2, P = 0; };
+template <> struct VariantCfg<float, 8> { static constexpr int V = 2, MINB = 5, NPF = 2, D = 2, P = 0; };
+template <> struct VariantCfg<float, 9> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 2, P = 1; };
+template <> struct VariantCfg<float, 10> { static constexpr int V = 4, MINB = 3, NPF = 3, D = 2, P = 1; };
+template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 1, P = 0; };
+template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 1, P = 0; };
+template <> struct VariantCfg<double, 2> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 1, P = 0; };
+template <> struct VariantCfg<double, 3> { static constexpr int V = 1, MINB = 4, NPF = 3, D = 1, P = 0; };
+template <> struct VariantCfg<double, 4> { static constexpr int V = 1, MINB = 5, NPF = 2, D = 1, P = 0; };
+template <> struct VariantCfg<double, 5> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 2, P = 0; };
+template <> struct VariantCfg<double, 6> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 2, P = 0; };
+template <> struct VariantCfg<double, 7> { static constexpr int V = 1, MINB = 3, NPF = 3, D = 2, P = 0; };
+template <> struct VariantCfg<double, 8> { static constexpr int V = 1, MINB = 5, NPF = 2, D = 2, P = 0; };
+template <> struct VariantCfg<double, 9> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 2, P = 1; };
+template <> struct VariantCfg<double, 10> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 2, P = 1; };
+constexpr int kVariants = 11;
 
 template <typename T, int VAR>
 struct VariantKernel {
   using C = VariantCfg<T, VAR>;
-  static void* fn() { return (void*)fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D>; }
+  static void* fn() {
+    if constexpr (C::P == 1)
+      return (void*)fused_pair_kernel<T, C::V, C::MINB, C::NPF>;
+    else
+      return (void*)fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D>;
+  }
   static size_t smem() {
-    return (size_t)kWarps * warp_elems<T, C::V, C::NPF, C::D>() * sizeof(T);
+    if constexpr (C::P == 1)
+      return (size_t)(kWarps / 2) * march::pair_smem_bytes<T, C::V, C::NPF>();
+    else
+      return (size_t)kWarps * warp_elems<T, C::V, C::NPF, C::D>() * sizeof(T);
   }
   // dynamic shared memory above 48 KB must be opted into once per kernel
   static void prepare() {
@@ -87,7 +129,10 @@ struct VariantKernel {
     }
   }
   static void launch(const FusedPlan& pl, const FusedParams<T>& p, cudaStream_t s) {
-    fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
+    if constexpr (C::P == 1)
+      fused_pair_kernel<T, C::V, C::MINB, C::NPF><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
+    else
+      fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
   }
 };
 
@@ -102,6 +147,8 @@ R with_variant(int var, A&&... a) {
     case 6: return Op<T, 6>::run(a...);
     case 7: return Op<T, 7>::run(a...);
     case 8: return Op<T, 8>::run(a...);
+    case 9: return Op<T, 9>::run(a...);
+    case 10: return Op<T, 10>::run(a...);
     default: return Op<T, 0>::run(a...);
   }
 }
@@ -113,6 +160,10 @@ struct LanesOp {
 template <typename T, int VAR>
 struct DepthOp {
   static int run() { return VariantCfg<T, VAR>::D; }
+};
+template <typename T, int VAR>
+struct PairOp {
+  static int run() { return VariantCfg<T, VAR>::P; }
 };
 template <typename T, int VAR>
 struct ResidentOp {
@@ -172,9 +223,11 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
   pl.variant = variant < 0 || variant >= kVariants ? 0 : variant;
   pl.lanes = fused_variant_lanes<T>(pl.variant);
   pl.depth = fused_variant_depth<T>(pl.variant);
+  pl.warps_per_task = with_variant<T, PairOp, int>(pl.variant) ? 2 : 1;
   const int out = pl.depth == 2 ? march::strip_cols2(pl.lanes) : strip_cols(pl.lanes);
   pl.nstrips = (nx + out - 1) / out;
-  int target = resident_warps > 0 ? kWaves * resident_warps / pl.nstrips : 1;
+  const int resident_tasks = resident_warps / pl.warps_per_task;
+  int target = resident_tasks > 0 ? kWaves * resident_tasks / pl.nstrips : 1;
   if (target < 1) target = 1;
   int seg = (ny + target - 1) / target;
   if (seg < min_seg * pl.depth) seg = min_seg * pl.depth;
@@ -183,7 +236,8 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
   pl.nsegs = (ny + seg - 1) / seg;
   pl.ntasks = pl.nstrips * pl.nsegs;
   pl.threads = kWarps * 32;
-  pl.blocks = (pl.ntasks + kWarps - 1) / kWarps;
+  const int tasks_per_block = kWarps / pl.warps_per_task;
+  pl.blocks = (pl.ntasks + tasks_per_block - 1) / tasks_per_block;
   pl.smem = with_variant<T, SmemOp, size_t>(pl.variant);
   return pl;
 }
@@ -191,9 +245,13 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
 template <typename T>
 cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pitch,
                               long long plane, const StepConsts<T>& c, int far_rot,
-                              const FusedPlan& plan, cudaStream_t s) {
+                              const FusedPlan& plan, int* status, unsigned long long wait_ns,
+                              cudaStream_t s) {
   if (plan.depth == 2 && far_rot) return cudaErrorInvalidValue;  // two steps assume clamped ends
+  if (plan.warps_per_task == 2 && status == nullptr) return cudaErrorInvalidValue;
   FusedParams<T> p;
+  p.status = status;
+  p.wait_ns = wait_ns;
   p.g = march::GridRef<T>{src, dst, nx, ny, pitch, plane, far_rot};
   p.nstrips = plan.nstrips;
   p.seg_len = plan.seg_len;
@@ -210,8 +268,8 @@ cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pi
   template int fused_resident_warps<T>(int, int);                                               \
   template FusedPlan plan_fused<T>(int, int, int, int, int);                                    \
   template cudaError_t launch_fused_step<T>(const T*, T*, int, int, long long, long long,       \
-                                            const StepConsts<T>&, int, const FusedPlan&,        \
-                                            cudaStream_t);
+                                            const StepConsts<T>&, int, const FusedPlan&, int*,  \
+                                            unsigned long long, cudaStream_t);
 LE2D_INST(float)
 LE2D_INST(double)
 #undef LE2D_INST
