@@ -61,23 +61,26 @@ int le2d_step_n(le_task *task, int nsteps);
  * stream, synchronised), in milliseconds. */
 int le2d_step_n_timed(le_task *task, int nsteps, float *ms);
 
-/* Step kernels: FUSED = one kernel per step (x- and y-sweep fused per strip);
+/* Step kernels: FUSED = x- and y-sweep fused per strip, one or two steps per launch;
  * SPLIT = the plain scheme, one kernel per sweep. */
 #define LE2D_METHOD_FUSED 0
 #define LE2D_METHOD_SPLIT 1
 int le2d_set_method(le_task *task, int method);
 
 /* Fused-kernel variant (columns per lane / register bound / input-ring depth / temporal-block
- * depth; -1 = default) and row segment length (0 = fill the device once) for this task's
- * grid.  A variant of temporal-block depth 2 advances two steps per launch; odd step counts
- * and le_step_soa then take single steps. */
+ * depth / warp pair; -1 = default) and row segment length (0 = the planner's) for this
+ * task's grid.  A variant of temporal-block depth 2 advances two steps per launch; odd step
+ * counts and le_step_soa then take single steps.  On a warp-pair variant a wait between the
+ * two warps of a tile that runs out (a fault, not a slow partner) is reported as
+ * LE2D_ETIMEOUT at the next synchronisation (le2d_wait, le2d_download, le2d_sync_host). */
 int le2d_set_variant(le_task *task, int variant, int seg_len);
-/* out[7] = {variant, columns per lane, segment rows, strips, warp tasks, blocks,
- * temporal-block depth}. */
+/* out[8] = {variant, columns per lane, segment rows, strips, tiles, blocks,
+ * temporal-block depth, warps per tile (2: producer / consumer warp pair)}. */
 int le2d_get_plan(const le_task *task, int *out);
 
 /* Autotuner: times every compiled fused-kernel variant (columns per lane, register bound,
- * row-loop unroll) and row-segment length on a scratch state of nx x ny nodes, and keeps
+ * input-ring depth, temporal-block depth, warp pair) and row-segment length on a scratch
+ * state of nx x ny nodes, and keeps
  * the fastest for the size class (nx, ny rounded up to powers of two).  Tasks created
  * afterwards in that class use it; with LE2D_AUTOTUNE=1 le_init_task tunes a class on its
  * first task.  out_plan (may be NULL) as le2d_get_plan; *nu_per_s (may be NULL) = the

@@ -252,7 +252,7 @@ class Lib:
     def set_variant(self, t, variant: int, seg_len: int = 0) -> int:
         return self.lib.le2d_set_variant(ctypes.byref(t), variant, seg_len)
 
-    PLAN_KEYS = ("variant", "lanes", "seg_len", "nstrips", "ntasks", "blocks", "depth")
+    PLAN_KEYS = ("variant", "lanes", "seg_len", "nstrips", "ntasks", "blocks", "depth", "warps_per_task")
 
     def get_plan(self, t) -> dict:
         out = (ctypes.c_int * len(self.PLAN_KEYS))()

@@ -45,6 +45,7 @@ struct DevTask {
   double* d_diag = nullptr;
   int* d_status = nullptr;    // set by a warp-pair launch whose wait gave up
   bool pairs_queued = false;  // warp-pair launches since d_status was last read
+  int stall_pair = -1;        // test hook (LE2D_TEST_STALL_PAIR): tile whose producer stalls
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   bool pinned = false;     // task->grid from cudaHostAlloc
@@ -333,8 +334,12 @@ cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int meth
   const bool two = d->plan.depth == 2 && max_steps >= 2 && !far_rot;
   const FusedPlan& pl = two ? d->plan : d->plan1;
   if (pl.warps_per_task == 2) d->pairs_queued = true;
+  le2d::PairCtl pc;
+  pc.status = d->d_status;
+  pc.wait_ns = kPairWaitNs;
+  pc.stall_task = d->stall_pair;
   cudaError_t e = le2d::launch_fused_step<T>(a, b, d->nx, d->ny, d->pitch, d->plane, c, far_rot,
-                                             pl, d->d_status, kPairWaitNs, d->stream);
+                                             pl, pc, d->stream);
   *cur ^= 1;
   *done += pl.depth;
   return e;
@@ -550,6 +555,9 @@ void le_init_task(le_task* task, const real dt, const le_vec2 h, const le_materi
         record(d, LE2D_ECUDA, "le_init_task: device setup", e);
         d->has_device = false;
       }
+      // Test hook for the bounded waits of warp-pair tiles: the producer of this tile
+      // hands nothing over, so the step ends with a timeout status instead of results.
+      if (const char* st = getenv("LE2D_TEST_STALL_PAIR")) d->stall_pair = atoi(st);
       Tuned tp;
       if (tuned_plan(n.x, n.y, &tp))
         replan(d, tp.variant, tp.seg_len);
@@ -771,6 +779,7 @@ int le2d_autotune(int nx, int ny, int* out_plan, double* nu_per_s) {
     const int tpb = p.threads / 32 / p.warps_per_task;  // tiles per block
     out_plan[5] = (out_plan[4] + tpb - 1) / tpb;
     out_plan[6] = p.depth;
+    out_plan[7] = p.warps_per_task;
   }
   return LE2D_OK;
 }
@@ -792,6 +801,7 @@ int le2d_get_plan(const le_task* task, int* out) {
   out[4] = d->plan.ntasks;
   out[5] = d->plan.blocks;
   out[6] = d->plan.depth;
+  out[7] = d->plan.warps_per_task;
   return LE2D_OK;
 }
 

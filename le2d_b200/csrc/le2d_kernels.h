@@ -40,14 +40,21 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
 template <typename T>
 int fused_resident_warps(int device, int variant);
 
+// Warp-pair plans: every wait between the warps of a pair is bounded by wait_ns, after
+// which the warp sets *status (a device int) and leaves.  stall_task >= 0 is a test hook:
+// the producer warp of that tile hands nothing over, so its partner's wait runs out.
+struct PairCtl {
+  int* status = nullptr;
+  unsigned long long wait_ns = 0;
+  int stall_task = -1;
+};
+
 // One fused launch src -> dst: plan.depth time steps.  far_rot selects the le_step_soa
-// far-end rows (depth-1 plans only).  Warp-pair plans bound every wait between the warps
-// of a pair by wait_ns and set *status (a device int) if one gave up.
+// far-end rows (depth-1 plans only).
 template <typename T>
 cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pitch,
                               long long plane, const StepConsts<T>& c, int far_rot,
-                              const FusedPlan& plan, int* status, unsigned long long wait_ns,
-                              cudaStream_t s);
+                              const FusedPlan& plan, const PairCtl& pair, cudaStream_t s);
 
 // The plain scheme: one sweep (axis 0 = x, 1 = y) src -> dst, one thread per node, the
 // reference's tvd2 formula node by node (two divisions per invariant).

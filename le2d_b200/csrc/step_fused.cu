@@ -19,8 +19,7 @@ struct FusedParams {
   march::GridRef<T> g;
   int nstrips, seg_len, ntasks;
   StepConsts<T> c;
-  int* status;                 // warp pairs: set when a wait gave up
-  unsigned long long wait_ns;  // warp pairs: bound of every wait
+  PairCtl pair;  // warp-pair waits
 };
 
 constexpr int kWarps = 4;  // warps per block
@@ -64,15 +63,16 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) fused_pair_kernel(const Fus
   __syncthreads();
   const int task = blockIdx.x * kPairs + pair;
   if (task >= p.ntasks) return;  // both warps of the pair
+  if (task == p.pair.stall_task && (wib & 1) == 0) return;  // test hook
   const int strip = task % p.nstrips;
   const int seg = task / p.nstrips;
   const int y0 = seg * p.seg_len;
   const int y1 = min(y0 + p.seg_len, p.g.ny);
   T* smem = reinterpret_cast<T*>(base);
   if ((wib & 1) == 0)
-    march::pair_produce<T, V, NPF>(p.g, p.c, strip, y0, y1, smem, bars, p.wait_ns, p.status);
+    march::pair_produce<T, V, NPF>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns, p.pair.status);
   else
-    march::pair_consume<T, V, NPF>(p.g, p.c, strip, y0, y1, smem, bars, p.wait_ns, p.status);
+    march::pair_consume<T, V, NPF>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns, p.pair.status);
 }
 
 // Compiled variants: columns per lane V (one 16- or 8-byte access per field), the
@@ -245,13 +245,11 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
 template <typename T>
 cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pitch,
                               long long plane, const StepConsts<T>& c, int far_rot,
-                              const FusedPlan& plan, int* status, unsigned long long wait_ns,
-                              cudaStream_t s) {
+                              const FusedPlan& plan, const PairCtl& pair, cudaStream_t s) {
   if (plan.depth == 2 && far_rot) return cudaErrorInvalidValue;  // two steps assume clamped ends
-  if (plan.warps_per_task == 2 && status == nullptr) return cudaErrorInvalidValue;
+  if (plan.warps_per_task == 2 && pair.status == nullptr) return cudaErrorInvalidValue;
   FusedParams<T> p;
-  p.status = status;
-  p.wait_ns = wait_ns;
+  p.pair = pair;
   p.g = march::GridRef<T>{src, dst, nx, ny, pitch, plane, far_rot};
   p.nstrips = plan.nstrips;
   p.seg_len = plan.seg_len;
@@ -268,8 +266,8 @@ cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pi
   template int fused_resident_warps<T>(int, int);                                               \
   template FusedPlan plan_fused<T>(int, int, int, int, int);                                    \
   template cudaError_t launch_fused_step<T>(const T*, T*, int, int, long long, long long,       \
-                                            const StepConsts<T>&, int, const FusedPlan&, int*,  \
-                                            unsigned long long, cudaStream_t);
+                                            const StepConsts<T>&, int, const FusedPlan&,        \
+                                            const PairCtl&, cudaStream_t);
 LE2D_INST(float)
 LE2D_INST(double)
 #undef LE2D_INST

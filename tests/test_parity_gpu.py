@@ -338,3 +338,40 @@ def test_full_size_8192_windows(libs, prec):
         wins.append((min(max(0, x0), p.nx - 192), min(max(0, y0), p.ny - 192), 192, 192))
     wins += [(0, 0, 160, 160), (p.nx - 130, 4000, 130, 150), (3000, p.ny - 140, 170, 140)]
     _window_parity(libs[prec], prec, p, 12, wins)
+
+
+def test_pair_bounded_wait_gives_up(libs, monkeypatch):
+    """Two-step tiles on warp pairs: a producer warp that never hands its rows over (test
+    hook LE2D_TEST_STALL_PAIR) makes its partner's bounded wait run out; the step reports
+    LE2D_ETIMEOUT at the next synchronisation and the device stays usable."""
+    lib = libs["f"]
+    pair = [v for v in variants(lib) if v in (9, 10)]
+    c = dict(nx=300, ny=200, hx=1.0, hy=1.0, c1=2.0, c2=1.0, rho=1.0, dt=0.25, stype=ST_AOS)
+    rng = np.random.default_rng(5)
+    g0 = rng.uniform(-1, 1, size=5 * 300 * 200).astype(lib.dtype)
+    monkeypatch.setenv("LE2D_TEST_STALL_PAIR", "0")
+    t = make_task(lib, c)
+    try:
+        assert lib.set_variant(t, pair[0], 0) == 0
+        assert lib.get_plan(t)["warps_per_task"] == 2
+        assert lib.upload(t, g0.copy()) == 0
+        assert lib.step_n(t, 2) == 0
+        assert lib.wait(t) == capi.LE2D_ETIMEOUT
+        assert lib.last_error(t) == capi.LE2D_ETIMEOUT
+    finally:
+        lib.le_free_task(t)
+    monkeypatch.delenv("LE2D_TEST_STALL_PAIR")
+    outs = []
+    for var in (pair[0], 2):
+        t = make_task(lib, c)
+        try:
+            assert lib.set_variant(t, var, 0) == 0
+            assert lib.upload(t, g0.copy()) == 0
+            assert lib.step_n(t, 6) == 0
+            o = np.zeros_like(g0)
+            assert lib.download(t, o) == 0
+            assert lib.last_error(t) == 0
+            outs.append(o)
+        finally:
+            lib.le_free_task(t)
+    assert outs[0].tobytes() == outs[1].tobytes()
