@@ -39,13 +39,15 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
   asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
                : "memory");
 }
+// Tests for the completion of the phase with parity `parity`; while it is incomplete the
+// thread is suspended (it issues nothing) until the phase completes or about 0.5 ms pass.
 __device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
   unsigned ok;
   asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(500000u)
       : "memory");
   return ok != 0;
 }
