@@ -18,7 +18,18 @@
 // `wait_ns` of global time (or once another warp has given up) the warp sets
 // ctl->status and leaves; the host reads the status (LE2D_ETIMEOUT), the context stays
 // usable.  State loads use ld.global.cg: other warps of this launch write them.
-#include "march.cuh"
+//
+// FP32 items advance two steps (temporal blocking) on a producer / consumer warp pair
+// (march_pair.cuh): the producer claims the item, passes its index to the consumer through
+// the pair's queue, waits for the item's dependencies, reads the state and runs the first
+// step; the consumer runs the second step on the rows it is handed, writes them and
+// publishes the tile.  The last item of an odd step count, and every item of an
+// le_step_soa instance, advances one step on the producer alone, which then publishes.
+// A producer may claim its next item while its consumer still finishes the last one: all
+// rows of that item are already in the queue, so the consumer finishes without it.
+#include <type_traits>
+
+#include "march_pair.cuh"
 
 namespace le2d {
 
@@ -109,15 +120,94 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
   }
 }
 
+template <typename T, int V, int MINB>
+__global__ void __launch_bounds__(kWarps * 32, MINB)
+    batch_pair_kernel(const BatchInst<T>* __restrict__ insts, const BatchTile* __restrict__ tiles,
+                      const long long* __restrict__ step_items, int nsteps, int* done,
+                      BatchCtl* ctl, unsigned long long wait_ns, int stall_plus1) {
+  using march::kHand;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const bool producer = (wib & 1) == 0;
+  unsigned char* base = smem_raw + (wib >> 1) * march::pair_smem_bytes<T, V, kNpf>();
+  T* smem = reinterpret_cast<T*>(base);
+  unsigned long long* bars =
+      reinterpret_cast<unsigned long long*>(base + march::pair_smem_elems<T, V, kNpf>() * sizeof(T));
+  volatile long long* item_q = reinterpret_cast<volatile long long*>(bars + 2 * kHand);
+  if (producer) march::pair_init<T, V>(bars);
+  __syncthreads();
+  const long long total = step_items[nsteps];
+  int* status = &ctl->status;
+  unsigned u = 0;  // handoffs through the pair's queue (item indices and rows)
+  int r = 0;
+  while (true) {
+    long long q;
+    const int hs = (int)(u % kHand);
+    if (producer) {
+      unsigned long long claimed = 0;
+      if (lane == 0) claimed = atomicAdd(&ctl->next, 1ULL);
+      q = (long long)__shfl_sync(0xffffffffu, claimed, 0);
+      const unsigned use = u / kHand;
+      if (use > 0 && !march::mbar_wait(bars + kHand + hs, (use - 1) & 1, wait_ns, status)) break;
+      if (lane == 0) item_q[hs] = q;
+      march::mbar_arrive(bars + hs);
+    } else {
+      if (!march::mbar_wait(bars + hs, (u / kHand) & 1, wait_ns, status)) break;
+      q = item_q[hs];
+      march::mbar_arrive(bars + kHand + hs);
+    }
+    ++u;
+    if (q >= total) break;
+    while (q >= step_items[r + 1]) ++r;
+    const BatchTile bt = tiles[q - step_items[r]];
+    const BatchInst<T>& I = insts[bt.inst];
+    const int nadv = min(I.depth, I.steps - r * I.depth);  // steps this item advances
+    if (!producer && nadv == 1) continue;  // the producer advances one-step items alone
+    if (producer && r > 0 &&
+        !wait_neighbours(done, I.tile_base, I.nstrips, I.nsegs, bt.seg, bt.strip, r, ctl, wait_ns))
+      break;
+    const int par = (I.parity + r) & 1;
+    const march::GridRef<T> g{I.buf[par], I.buf[par ^ 1], I.nx, I.ny, I.pitch, I.plane, I.far_rot};
+    const int y0 = bt.seg * I.seg_len;
+    const int y1 = min(y0 + I.seg_len, I.ny);
+    // absolute step count the rows this warp writes (or hands over) complete
+    const long long after = I.abs_step0 + (long long)r * I.depth + (producer ? 1 : 2);
+    march::RowTap<T> tap{nullptr, -1};
+    if (I.trace != nullptr && after % I.trace_every == 0)
+      tap = march::RowTap<T>{I.trace + (after / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
+    const bool ok =
+        producer ? march::pair_produce<T, V, kNpf, true, true>(g, I.c, bt.strip, y0, y1, smem, bars,
+                                                               wait_ns, status, u, nadv == 1, tap)
+                 : march::pair_consume<T, V, kNpf, true>(g, I.c, bt.strip, y0, y1, smem, bars,
+                                                         wait_ns, status, u, tap);
+    if (!ok) break;
+    if (producer == (nadv == 1)) {  // the warp that wrote the tile's new state publishes it
+      __syncwarp();
+      const int tile_id = I.tile_base + bt.seg * I.nstrips + bt.strip;
+      if (lane == 0 && !(r == 0 && tile_id == stall_plus1 - 1)) {
+        __threadfence();
+        st_release(done + tile_id, r + 1);
+      }
+    }
+  }
+}
+
 template <typename T>
 struct BatchKernelOf;
+// FP32: two-step items on warp pairs (4 columns per lane, 16 warps per SM); FP64: one-step
+// items on single warps (2 columns per lane).
 template <>
 struct BatchKernelOf<float> {
-  static constexpr int V = 4, MINB = 3;
+  static constexpr int V = 4, MINB = 3, DEPTH = 2;
+  static void* fn() { return (void*)batch_pair_kernel<float, V, MINB>; }
+  static size_t smem() { return (size_t)(kWarps / 2) * march::pair_smem_bytes<float, V, kNpf>(); }
 };
 template <>
 struct BatchKernelOf<double> {
-  static constexpr int V = 2, MINB = 2;
+  static constexpr int V = 2, MINB = 2, DEPTH = 1;
+  static void* fn() { return (void*)batch_kernel<double, V, MINB>; }
+  static size_t smem() { return (size_t)kWarps * march::warp_smem_elems<double, V, kNpf>() * sizeof(double); }
 };
 
 }  // namespace
@@ -126,20 +216,20 @@ template <typename T>
 int batch_lanes() { return BatchKernelOf<T>::V; }
 
 template <typename T>
-size_t batch_smem() {
-  return (size_t)kWarps * march::warp_smem_elems<T, BatchKernelOf<T>::V, kNpf>() * sizeof(T);
-}
+int batch_depth() { return BatchKernelOf<T>::DEPTH; }
+
+template <typename T>
+size_t batch_smem() { return BatchKernelOf<T>::smem(); }
 
 template <typename T>
 int batch_resident_blocks(int device) {
   using K = BatchKernelOf<T>;
   int sms = 0, per_sm = 0;
   // dynamic shared memory above 48 KB is opted into once (before any launch or capture)
-  cudaFuncSetAttribute(batch_kernel<T, K::V, K::MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)batch_smem<T>());
+  cudaFuncSetAttribute(K::fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_smem<T>());
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<T, K::V, K::MINB>,
-                                                    kWarps * 32, batch_smem<T>()) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, K::fn(), kWarps * 32, batch_smem<T>()) !=
+      cudaSuccess)
     return 0;
   return sms * per_sm;
 }
@@ -150,16 +240,22 @@ cudaError_t launch_batch(const BatchInst<T>* insts, const BatchTile* tiles,
                          BatchCtl* ctl, unsigned long long wait_ns, int stall_plus1,
                          int resident_blocks, cudaStream_t s) {
   using K = BatchKernelOf<T>;
-  long long blocks = (total_items + kWarps - 1) / kWarps;
-  if (blocks > resident_blocks) blocks = resident_blocks;
+  const int per_block = K::DEPTH == 2 ? kWarps / 2 : kWarps;  // items a block works on at once
+  long long blocks = (total_items + per_block - 1) / per_block;
+  if (blocks > resident_blocks) blocks = resident_blocks;  // persistent: all blocks resident
   if (blocks < 1) blocks = 1;
-  batch_kernel<T, K::V, K::MINB><<<(int)blocks, kWarps * 32, batch_smem<T>(), s>>>(
-      insts, tiles, step_items, nsteps, done, ctl, wait_ns, stall_plus1);
+  if constexpr (K::DEPTH == 2)
+    batch_pair_kernel<T, K::V, K::MINB><<<(int)blocks, kWarps * 32, batch_smem<T>(), s>>>(
+        insts, tiles, step_items, nsteps, done, ctl, wait_ns, stall_plus1);
+  else
+    batch_kernel<T, K::V, K::MINB><<<(int)blocks, kWarps * 32, batch_smem<T>(), s>>>(
+        insts, tiles, step_items, nsteps, done, ctl, wait_ns, stall_plus1);
   return cudaGetLastError();
 }
 
 #define LE2D_INST(T)                                                                            \
   template int batch_lanes<T>();                                                                \
+  template int batch_depth<T>();                                                                \
   template size_t batch_smem<T>();                                                              \
   template int batch_resident_blocks<T>(int);                                                   \
   template cudaError_t launch_batch<T>(const BatchInst<T>*, const BatchTile*, const long long*, \

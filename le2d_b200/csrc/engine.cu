@@ -161,6 +161,11 @@ int Engine<T>::add(const le2d_problem& p, const T* init, int ndisks, const T* di
   in.buf[0] = reinterpret_cast<T*>(arena_->base() + in.state_off);
   in.buf[1] = in.buf[0] + 5 * in.plane;
   in.c = problem_consts<T>(p);
+  // le_step_soa's far end is not a clamp: its instances advance one step per work item
+  in.depth = p.stype == ST_AOS ? batch_depth<T>() : 1;
+  // one- and two-step tiles have the same strips at the two-step kernel's 4 columns per
+  // lane (one halo lane per side for either)
+  static_assert(strip_cols(4) == strip_cols2(4), "strip widths of one and two steps");
   const int out = strip_cols(batch_lanes<T>());
   in.nstrips = (p.nx + out - 1) / out;
   in.seg_len = std::min(seg_len_, p.ny);
@@ -191,16 +196,18 @@ int Engine<T>::add(const le2d_problem& p, const T* init, int ndisks, const T* di
 }
 
 template <typename T>
-typename Engine<T>::Window Engine<T>::plan_window(int window,
-                                                  const std::vector<long long>& done) const {
+typename Engine<T>::Window Engine<T>::plan_window(int window, const std::vector<long long>& done,
+                                                  const std::vector<int>& cur) const {
   Window w;
-  std::vector<std::pair<int, int>> order;  // (steps in window, id)
+  std::vector<std::pair<int, int>> order;  // (work-item steps in window, id)
+  std::vector<int> steps_of(insts_.size(), 0);
   for (int id = 0; id < (int)insts_.size(); ++id) {
     const Inst& in = insts_[id];
     if (!in.live) continue;
     const long long left = in.p.steps - done[id];
     if (left <= 0) continue;
-    order.push_back({(int)std::min<long long>(left, window), id});
+    steps_of[id] = (int)std::min<long long>(left, window);
+    order.push_back({(steps_of[id] + in.depth - 1) / in.depth, id});
   }
   std::stable_sort(order.begin(), order.end(),
                    [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
@@ -222,15 +229,17 @@ typename Engine<T>::Window Engine<T>::plan_window(int window,
     b.nsegs = in.nsegs;
     b.seg_len = in.seg_len;
     b.tile_base = tile_base;
-    b.parity = (int)(done[order[k].second] & 1);
-    b.steps = order[k].first;
+    b.parity = cur[order[k].second];
+    b.steps = steps_of[order[k].second];
+    b.depth = in.depth;
     b.abs_step0 = done[order[k].second];
     b.trace = in.trace;
     b.trace_row = in.trace ? in.p.receiver_row : -1;
     b.trace_every = in.trace ? in.p.receiver_every : 1;
     w.insts.push_back(b);
     w.inst_ids.push_back(order[k].second);
-    w.inst_steps.push_back(order[k].first);
+    w.inst_steps.push_back(steps_of[order[k].second]);
+    w.inst_items.push_back(order[k].first);
     for (int s = 0; s < in.nsegs; ++s)
       for (int st = 0; st < in.nstrips; ++st) w.tiles.push_back(BatchTile{(int)k, st, s, 0});
     tile_base += in.nstrips * in.nsegs;
@@ -287,8 +296,12 @@ int Engine<T>::run_window(int window) {
   if (!ok()) return LE2D_ENODEV;
   if (window < 1) return LE2D_EINVAL;
   std::vector<long long> done(insts_.size());
-  for (size_t i = 0; i < insts_.size(); ++i) done[i] = insts_[i].done_steps;
-  Window w = plan_window(window, done);
+  std::vector<int> cur(insts_.size());
+  for (size_t i = 0; i < insts_.size(); ++i) {
+    done[i] = insts_[i].done_steps;
+    cur[i] = insts_[i].cur;
+  }
+  Window w = plan_window(window, done, cur);
   if (w.steps == 0) return LE2D_OK;
   int rc = ensure_scratch(w.insts.size(), w.tiles.size(), w.step_items.size(), w.tiles.size(), 1);
   if (rc) return rc;
@@ -311,6 +324,7 @@ int Engine<T>::run_window(int window) {
   for (size_t k = 0; k < w.inst_ids.size(); ++k) {
     Inst& in = insts_[w.inst_ids[k]];
     in.done_steps += w.inst_steps[k];
+    in.cur ^= w.inst_items[k] & 1;  // each work-item step writes the other buffer
     node_updates_ += (long long)in.p.nx * in.p.ny * w.inst_steps[k];
   }
   return LE2D_OK;
@@ -321,13 +335,20 @@ int Engine<T>::run_all(int window, float* ms) {
   if (!ok()) return LE2D_ENODEV;
   if (window < 1) return LE2D_EINVAL;
   std::vector<long long> done(insts_.size());
-  for (size_t i = 0; i < insts_.size(); ++i) done[i] = insts_[i].done_steps;
+  std::vector<int> cur(insts_.size());
+  for (size_t i = 0; i < insts_.size(); ++i) {
+    done[i] = insts_[i].done_steps;
+    cur[i] = insts_[i].cur;
+  }
   std::vector<Window> ws;
   size_t ni = 0, nt = 0, nitems = 0;
   while (true) {
-    Window w = plan_window(window, done);
+    Window w = plan_window(window, done, cur);
     if (w.steps == 0) break;
-    for (size_t k = 0; k < w.inst_ids.size(); ++k) done[w.inst_ids[k]] += w.inst_steps[k];
+    for (size_t k = 0; k < w.inst_ids.size(); ++k) {
+      done[w.inst_ids[k]] += w.inst_steps[k];
+      cur[w.inst_ids[k]] ^= w.inst_items[k] & 1;
+    }
     ni += w.insts.size();
     nt += w.tiles.size();
     nitems += w.step_items.size();
@@ -392,6 +413,7 @@ int Engine<T>::run_all(int window, float* ms) {
     for (size_t k = 0; k < w.inst_ids.size(); ++k) {
       Inst& in = insts_[w.inst_ids[k]];
       in.done_steps += w.inst_steps[k];
+      in.cur ^= w.inst_items[k] & 1;
       node_updates_ += (long long)in.p.nx * in.p.ny * w.inst_steps[k];
     }
   return LE2D_OK;
@@ -407,7 +429,7 @@ int Engine<T>::fields(int id, T* out) {
   if (id < 0 || id >= (int)insts_.size() || !out) return LE2D_EINVAL;
   const Inst& in = insts_[id];
   if (!in.live) return LE2D_ESTATE;
-  const int cur = (int)(in.done_steps & 1);
+  const int cur = in.cur;
   cudaError_t e = launch_unpack<T>(in.buf[cur], in.buf[cur ^ 1], in.p.nx, in.p.ny, in.pitch,
                                    in.plane, in.p.stype == ST_AOS, stream_);
   if (e == cudaSuccess)
@@ -442,7 +464,7 @@ int Engine<T>::diagnostics(int id, le2d_diag_t* out) {
   double h[11];
   cudaError_t e = cudaMemsetAsync(d_diag_, 0, 11 * sizeof(double), stream_);
   if (e == cudaSuccess)
-    e = launch_diag<T>(in.buf[in.done_steps & 1], in.p.nx, in.p.ny, in.pitch, in.plane, rho,
+    e = launch_diag<T>(in.buf[in.cur], in.p.nx, in.p.ny, in.pitch, in.plane, rho,
                        (la + 2.0 * mu) / (8.0 * mu * (la + mu)), -2.0 * la / (8.0 * mu * (la + mu)),
                        1.0 / (2.0 * mu), d_diag_, stream_);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h, d_diag_, sizeof(h), cudaMemcpyDeviceToHost, stream_);

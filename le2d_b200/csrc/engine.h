@@ -46,6 +46,8 @@ class Engine {
     T* trace = nullptr;
     int nsamples = 0;
     long long done_steps = 0;
+    int cur = 0;    // buffer holding the current state
+    int depth = 1;  // steps per work item of the batched kernel
     StepConsts<T> c;
     int nstrips = 0, nsegs = 0, seg_len = 0;
     bool live = false;
@@ -85,10 +87,13 @@ class Engine {
     std::vector<BatchTile> tiles;
     std::vector<long long> step_items;  // size steps+1
     std::vector<int> inst_ids;
-    std::vector<int> inst_steps;
-    int steps = 0;
+    std::vector<int> inst_steps;  // time steps of each instance in the window
+    std::vector<int> inst_items;  // work-item steps of each instance (ceil(steps / depth))
+    int steps = 0;                // work-item steps of the window
   };
-  Window plan_window(int window, const std::vector<long long>& done_steps) const;
+  // done_steps / cur: each instance's steps so far and current buffer before the window.
+  Window plan_window(int window, const std::vector<long long>& done_steps,
+                     const std::vector<int>& cur) const;
   int ensure_scratch(size_t insts, size_t tiles, size_t items, size_t done, size_t ctls);
   int launch_window(const Window& w, size_t inst_off, size_t tile_off, size_t item_off,
                     size_t done_off, size_t ctl_off);

@@ -15,6 +15,10 @@ namespace le2d {
 // the outermost halo_lanes() lanes on each side only supply neighbours.
 __host__ __device__ constexpr int halo_lanes(int lanes) { return lanes >= 2 ? 1 : 2; }
 __host__ __device__ constexpr int strip_cols(int lanes) { return (32 - 2 * halo_lanes(lanes)) * lanes; }
+// Two steps per tile: the second step's stencil reaches 4 nodes each way from the strip's
+// edge, so ceil(4 / lanes) halo lanes per side.
+__host__ __device__ constexpr int halo_lanes2(int lanes) { return (4 + lanes - 1) / lanes; }
+__host__ __device__ constexpr int strip_cols2(int lanes) { return (32 - 2 * halo_lanes2(lanes)) * lanes; }
 
 struct FusedPlan {
   int variant = 0, lanes = 0;
@@ -90,6 +94,8 @@ struct BatchInst {
   int tile_base;         // index of the instance's first tile in the tile list and done[]
   int parity;            // buffer holding the state at window step 0
   int steps;             // steps of this instance in the window
+  int depth;             // steps per work item (temporal-block depth); the last item of an
+                         // odd step count advances one step
   long long abs_step0;   // steps the instance had done before the window
   T* trace;              // receiver samples [sample][2][pitch], or null
   int trace_row;         // receiver row
@@ -108,11 +114,16 @@ struct BatchCtl {
 
 template <typename T>
 int batch_lanes();
+// Temporal-block depth of the batched kernel for clamped-end (le_step) instances: 2 for
+// FP32 (producer / consumer warp pairs), 1 for FP64; le_step_soa instances use 1.
+template <typename T>
+int batch_depth();
 template <typename T>
 size_t batch_smem();
 template <typename T>
 int batch_resident_blocks(int device);
-// step_items[r] = work items before window step r (r = 0..nsteps); done[] and ctl zeroed.
+// step_items[r] = work items before window item step r (r = 0..nsteps; an item step
+// advances each instance by its depth); done[] and ctl zeroed.
 // stall_plus1 > 0 is a test hook: tile (stall_plus1 - 1) never publishes its first step,
 // so the waits that depend on it run out and the launch ends with ctl->status = 1.
 template <typename T>

@@ -29,11 +29,6 @@ __host__ __device__ constexpr int warp_smem_elems2() {
   return (6 + NPF) * NF * 32 * V;  // input ring + step A ring + step B ring
 }
 
-__host__ __device__ constexpr int halo_lanes2(int lanes) { return (4 + lanes - 1) / lanes; }
-__host__ __device__ constexpr int strip_cols2(int lanes) {
-  return (32 - 2 * halo_lanes2(lanes)) * lanes;
-}
-
 template <typename T, int V>
 __device__ __forceinline__ T pick(const T (&a)[V], int i) {
   T s = a[0];

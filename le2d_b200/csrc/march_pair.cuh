@@ -80,14 +80,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 
 // Shared memory of one pair: the producer's input ring (NPF rows) and step-A ring (3),
 // the queue (kHand), the consumer's step-B ring (3), each row NF x 32V elements; then
-// 2 * kHand mbarriers.
+// 2 * kHand mbarriers and kHand 8-byte words a persistent kernel passes work items in.
 template <typename T, int V, int NPF>
 __host__ __device__ constexpr int pair_smem_elems() {
   return (NPF + 3 + kHand + 3) * NF * 32 * V;
 }
 template <typename T, int V, int NPF>
 __host__ __device__ constexpr int pair_smem_bytes() {
-  return pair_smem_elems<T, V, NPF>() * (int)sizeof(T) + 2 * kHand * 8;
+  return pair_smem_elems<T, V, NPF>() * (int)sizeof(T) + 2 * kHand * 8 + kHand * 8;
 }
 
 // How many rows of step B's stencil step-A row ka stands for (tile rows [y0, y1)):
@@ -105,14 +105,29 @@ __device__ __forceinline__ void pair_init(unsigned long long* bars) {
     for (int i = 0; i < 2 * kHand; ++i) mbar_init(bars + i, 32);
 }
 
-// Producer warp: step A of strip `strip`, rows [y0, y1) of the tile.
-template <typename T, int V, int NPF>
-__device__ __forceinline__ void pair_produce(const GridRef<T>& g, const StepConsts<T>& c, int strip,
+// Writes vx and vy of a row into a receiver line (RowTap) for this lane's V columns.
+template <typename T, int V>
+__device__ __forceinline__ void tap_row(const RowTap<T>& tap, long long pitch, int col0,
+                                        const T (&f)[NF][V]) {
+  using VT = typename Vec<T, V>::type;
+  *reinterpret_cast<VT*>(tap.out + col0) = pack(f[VX]);
+  *reinterpret_cast<VT*>(tap.out + pitch + col0) = pack(f[VY]);
+}
+
+// Producer warp: step A of strip `strip`, rows [y0, y1) of the tile, handing its rows to
+// the consumer; `u` counts the queue's handoffs (it continues across tiles).  With
+// one_step the warp instead writes step A's rows [y0, y1) to g.dst itself (a tile that
+// advances one step: an odd last step, or le_step_soa's far end, which g.far_rot selects).
+// `tap` (TAP): receiver row of step A's rows.  Returns false if a wait gave up.
+template <typename T, int V, int NPF, bool COHERENT, bool TAP>
+__device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepConsts<T>& c, int strip,
                                              int y0, int y1, T* smem_pair,
                                              unsigned long long* bars,
-                                             unsigned long long wait_ns, int* status) {
+                                             unsigned long long wait_ns, int* status, unsigned& u,
+                                             bool one_step, const RowTap<T>& tap) {
   using VT = typename Vec<T, V>::type;
   static_assert(NPF >= 2, "the input ring needs at least the current and the next row");
+  static_assert(!COHERENT || V * sizeof(T) == 16, "coherent loads need 16-byte (L2-only) copies");
   constexpr int H2 = halo_lanes2(V);
   constexpr int kIn = 32 * V;
   constexpr int kOut = strip_cols2(V);
@@ -126,6 +141,8 @@ __device__ __forceinline__ void pair_produce(const GridRef<T>& g, const StepCons
   const int xs = strip * kOut - H2 * V;
   const int col0 = xs + lane * V;
   const bool interior = xs >= 0 && xs + kIn <= g.nx;
+  const bool writer = lane >= H2 && lane < 32 - H2 && col0 < g.nx;
+  const int mend = one_step ? y1 + 2 : y1 + 4;  // one step needs the raw rows up to y1+1 only
 
   YPipe<T, V> ya;
   ya.init();
@@ -133,15 +150,17 @@ __device__ __forceinline__ void pair_produce(const GridRef<T>& g, const StepCons
   for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(a_ring + 2 * kRow + k * kIn) = VT{};
 #pragma unroll
   for (int j = 0; j < NPF - 1; ++j)
-    fetch_row<T, V, false>(in_ring + j * kRow, g, source_row(y0 - 4 + j, g.ny, 0), col0, interior);
+    fetch_row<T, V, COHERENT>(in_ring + j * kRow, g, source_row(y0 - 4 + j, g.ny, g.far_rot), col0,
+                              interior);
   int islot = 0, aslot = 0;
-  unsigned u = 0;  // handoffs so far
-  for (int m = y0 - 4; m < y1 + 4; ++m) {
+  bool ok = true;
+  for (int m = y0 - 4; m < mend; ++m) {
     {
       const int mm = m + NPF - 1;
       const int ns = islot + NPF - 1 >= NPF ? islot - 1 : islot + NPF - 1;
-      if (mm < y1 + 4)
-        fetch_row<T, V, false>(in_ring + ns * kRow, g, source_row(mm, g.ny, 0), col0, interior);
+      if (mm < mend)
+        fetch_row<T, V, COHERENT>(in_ring + ns * kRow, g, source_row(mm, g.ny, g.far_rot), col0,
+                                  interior);
       else
         cp_async_commit();
     }
@@ -153,13 +172,28 @@ __device__ __forceinline__ void pair_produce(const GridRef<T>& g, const StepCons
     sweep_x_lane<T, V>(f, c.x);
     ring_left(ya, f, a_ring, aslot, c.y);
     const int ka = m - 2;  // step-A row completed now
-    if (m >= y0 && row_uses(ka, y0, y1, g.ny) > 0) {
+    if (one_step) {
+      if (m >= y0 + 2) {  // ka in [y0, y1)
+        T ga[NF][V];
+        ring_output(ya, ga, a_ring, aslot, c.y);
+        if (writer) {
+          T* out = g.dst + (long long)ka * g.pitch + col0;
+#pragma unroll
+          for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(out + k * g.plane) = pack(ga[k]);
+          if (TAP && ka == tap.row) tap_row<T, V>(tap, g.pitch, col0, ga);
+        }
+      }
+    } else if (m >= y0 && row_uses(ka, y0, y1, g.ny) > 0) {
       T ga[NF][V];
       ring_output(ya, ga, a_ring, aslot, c.y);
+      if (TAP && ka == tap.row && ka >= y0 && ka < y1 && writer) tap_row<T, V>(tap, g.pitch, col0, ga);
       if (!interior) clamp_columns<T, V>(ga, xs, col0, g.nx);
       const int hs = (int)(u % kHand);
       const unsigned use = u / kHand;
-      if (use > 0 && !mbar_wait(empty + hs, (use - 1) & 1, wait_ns, status)) break;
+      if (use > 0 && !mbar_wait(empty + hs, (use - 1) & 1, wait_ns, status)) {
+        ok = false;
+        break;
+      }
       T* slot = hand + hs * kRow;
 #pragma unroll
       for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(slot + k * kIn) = pack(ga[k]);
@@ -171,14 +205,17 @@ __device__ __forceinline__ void pair_produce(const GridRef<T>& g, const StepCons
     aslot = aslot == 2 ? 0 : aslot + 1;
   }
   cp_async_wait<0>();  // nothing of this warp's in flight when it leaves (also after a break)
+  return ok;
 }
 
-// Consumer warp: step B of the same tile, writing rows [y0, y1) to g.dst.
-template <typename T, int V, int NPF>
-__device__ __forceinline__ void pair_consume(const GridRef<T>& g, const StepConsts<T>& c, int strip,
+// Consumer warp: step B of the same tile, writing rows [y0, y1) to g.dst; `u` as for the
+// producer, `tap` (TAP): receiver row of step B's rows.  Returns false if a wait gave up.
+template <typename T, int V, int NPF, bool TAP>
+__device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepConsts<T>& c, int strip,
                                              int y0, int y1, T* smem_pair,
                                              unsigned long long* bars,
-                                             unsigned long long wait_ns, int* status) {
+                                             unsigned long long wait_ns, int* status, unsigned& u,
+                                             const RowTap<T>& tap) {
   using VT = typename Vec<T, V>::type;
   constexpr int H2 = halo_lanes2(V);
   constexpr int kIn = 32 * V;
@@ -199,12 +236,11 @@ __device__ __forceinline__ void pair_consume(const GridRef<T>& g, const StepCons
   for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(b_ring + 2 * kRow + k * kIn) = VT{};
   int bslot = 0;
   int bin = y0 - 2;  // step-B row index of the next row fed to step B
-  unsigned u = 0;
   for (int ka = y0 - 2; ka < y1 + 2; ++ka) {
     const int reps = row_uses(ka, y0, y1, g.ny);
     if (reps == 0) continue;
     const int hs = (int)(u % kHand);
-    if (!mbar_wait(full + hs, (u / kHand) & 1, wait_ns, status)) return;
+    if (!mbar_wait(full + hs, (u / kHand) & 1, wait_ns, status)) return false;
     const T* slot = hand + hs * kRow;
     for (int r = 0; r < reps; ++r) {  // the slot is read once per use, released after the last
       T fb[NF][V];
@@ -217,9 +253,11 @@ __device__ __forceinline__ void pair_consume(const GridRef<T>& g, const StepCons
         T gb[NF][V];
         ring_output(yb, gb, b_ring, bslot, c.y);
         if (writer) {
-          T* out = g.dst + (long long)(bin - 2) * g.pitch + col0;
+          const int row = bin - 2;
+          T* out = g.dst + (long long)row * g.pitch + col0;
 #pragma unroll
           for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(out + k * g.plane) = pack(gb[k]);
+          if (TAP && row == tap.row) tap_row<T, V>(tap, g.pitch, col0, gb);
         }
       }
       yb.right(c.y);
@@ -228,6 +266,7 @@ __device__ __forceinline__ void pair_consume(const GridRef<T>& g, const StepCons
     }
     ++u;
   }
+  return true;
 }
 
 }  // namespace march

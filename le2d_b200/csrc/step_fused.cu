@@ -69,10 +69,14 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) fused_pair_kernel(const Fus
   const int y0 = seg * p.seg_len;
   const int y1 = min(y0 + p.seg_len, p.g.ny);
   T* smem = reinterpret_cast<T*>(base);
+  unsigned u = 0;
+  const march::RowTap<T> no_tap{nullptr, -1};
   if ((wib & 1) == 0)
-    march::pair_produce<T, V, NPF>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns, p.pair.status);
+    march::pair_produce<T, V, NPF, false, false>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns,
+                                                 p.pair.status, u, false, no_tap);
   else
-    march::pair_consume<T, V, NPF>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns, p.pair.status);
+    march::pair_consume<T, V, NPF, false>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns,
+                                          p.pair.status, u, no_tap);
 }
 
 // Compiled variants: columns per lane V (one 16- or 8-byte access per field), the
@@ -224,7 +228,7 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
   pl.lanes = fused_variant_lanes<T>(pl.variant);
   pl.depth = fused_variant_depth<T>(pl.variant);
   pl.warps_per_task = with_variant<T, PairOp, int>(pl.variant) ? 2 : 1;
-  const int out = pl.depth == 2 ? march::strip_cols2(pl.lanes) : strip_cols(pl.lanes);
+  const int out = pl.depth == 2 ? strip_cols2(pl.lanes) : strip_cols(pl.lanes);
   pl.nstrips = (nx + out - 1) / out;
   const int resident_tasks = resident_warps / pl.warps_per_task;
   int target = resident_tasks > 0 ? kWaves * resident_tasks / pl.nstrips : 1;
