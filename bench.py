@@ -347,6 +347,18 @@ def run_batched(args):
             outs = [b.fields(i) for i in ids] if scale_steps is None else None
             return ms, wall, outs
 
+    # batched-path autotuner: tile height and steps per work item for every size class of the
+    # mix (outside the timed region; the table then applies to the instances added below)
+    tuned, tune_s = {}, 0.0
+    if not args.no_tune:
+        lib.batch_autotune_reset()
+        t0 = time.perf_counter()
+        for p in probs:
+            key = (max(p.nx - 1, 1).bit_length(), max(p.ny - 1, 1).bit_length())
+            if key not in tuned:
+                plan, nus = lib.batch_autotune(p.nx, p.ny)
+                tuned[key] = {**plan, "nu_s": nus}
+        tune_s = time.perf_counter() - t0
     batch_run(scale_steps=8)  # warm-up (kernels, allocations)
     ms, wall, outs = batch_run()
     # the plain loop: every instance alone, one le_step call per step
@@ -391,6 +403,7 @@ def run_batched(args):
                     "rho U[1,3], dt=0.5h/c1, 1-4 disks, steps U[200,2000]",
         "node_updates": nu, "batched_device_s": ms * 1e-3, "batched_wall_s": wall,
         "batched_nu_s": nu / (ms * 1e-3), "window_steps": args.window,
+        "autotune": {"seconds": tune_s, "classes": {f"2^{a}x2^{b}": v for (a, b), v in sorted(tuned.items())}},
         "plain_le_step_loop_s": plain_s, "plain_le_step_solves_s": len(probs) / plain_s,
         "plain_le_step_loop_steps_only_s": loop_only[0],
         "plain_step_n_loop_s": plain_n_s, "plain_step_n_solves_s": len(probs) / plain_n_s,
@@ -580,6 +593,7 @@ def main():
     ap.add_argument("--budget", type=int, default=48, help="serving: HBM budget in GiB")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 leg")
+    ap.add_argument("--no-tune", action="store_true", help="batched: skip the batched-path autotuner")
     ap.add_argument("--time-steps", type=int, default=None, help="time steps per solve (default 1000)")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -158,6 +158,16 @@ int le2d_batch_diagnostics(le2d_batch *b, int id, le2d_diag_t *out);
 /* Bounded dependency waits: the kernel gives up after this many ns (default 2e9) and
  * le2d_batch_run returns LE2D_ETIMEOUT. */
 int le2d_batch_set_wait_limit(le2d_batch *b, unsigned long long ns);
+/* Batched-path autotuner: times the batched kernel on copies of a scratch problem of
+ * nx x ny nodes (enough copies for ~24 M nodes) for every tile height (16 ... 256 rows) and
+ * steps per work item (1, and 2 -- a producer / consumer warp pair per tile -- in the FP32
+ * library), and keeps the fastest for the size class (nx, ny rounded up to powers of two).
+ * Instances of a tuned class that are added to a batch or a server afterwards use it; with
+ * LE2D_AUTOTUNE=1 le2d_batch_add tunes a class on its first instance.  out (may be NULL):
+ * {tile rows, steps per item}; *nu_per_s (may be NULL): the measured node-updates/s. */
+int le2d_batch_autotune(int nx, int ny, int *out, double *nu_per_s);
+/* Forgets every tuned size class of the batched path. */
+int le2d_batch_autotune_reset(void);
 
 /* ---- Served solves (continuous batching) --------------------------------------------
  * A background loop owns a device arena of `device_budget_bytes`.  Requests are queued

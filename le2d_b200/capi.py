@@ -46,6 +46,7 @@ EXPORTS = [
     "le2d_server_create", "le2d_server_destroy", "le2d_server_submit", "le2d_server_poll",
     "le2d_server_wait", "le2d_server_result", "le2d_server_times", "le2d_server_release",
     "le2d_server_stats", "le2d_now", "le2d_diagnostics_noalloc", "le2d_autotune", "le2d_autotune_reset",
+    "le2d_batch_autotune", "le2d_batch_autotune_reset",
 ]
 
 LE2D_DIAG_NOALLOC_MAX_ROWS = 16384
@@ -178,6 +179,8 @@ class Lib:
         L.le2d_now.restype = ctypes.c_double
         L.le2d_autotune.argtypes = [ctypes.c_int, ctypes.c_int, P(ctypes.c_int), P(ctypes.c_double)]
         L.le2d_autotune_reset.argtypes = []
+        L.le2d_batch_autotune.argtypes = [ctypes.c_int, ctypes.c_int, P(ctypes.c_int), P(ctypes.c_double)]
+        L.le2d_batch_autotune_reset.argtypes = []
         L.le2d_diagnostics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
                                                ctypes.c_longlong, R, R, R, R, R, ctypes.c_void_p,
                                                P(self.le2d_diag_t)]
@@ -271,6 +274,18 @@ class Lib:
 
     def autotune_reset(self) -> int:
         return self.lib.le2d_autotune_reset()
+
+    def batch_autotune(self, nx: int, ny: int):
+        """Tunes the batched path for the size class of nx x ny: ({seg_len, depth}, nu/s)."""
+        out = (ctypes.c_int * 2)()
+        nus = ctypes.c_double(0.0)
+        rc = self.lib.le2d_batch_autotune(nx, ny, out, ctypes.byref(nus))
+        if rc:
+            raise RuntimeError(self.strerror(rc))
+        return {"seg_len": out[0], "depth": out[1]}, nus.value
+
+    def batch_autotune_reset(self) -> int:
+        return self.lib.le2d_batch_autotune_reset()
 
     def sim_time(self, t):
         tt, st = ctypes.c_double(0.0), ctypes.c_longlong(0)

@@ -1,9 +1,11 @@
 // Batched solves: instance states in a device arena, per-window work lists for the
 // persistent kernel (batch.cu), CUDA-graph capture of the window loop, read-back.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <iterator>
+#include <mutex>
 
 #include "consts.h"
 #include "engine.h"
@@ -127,6 +129,98 @@ template <typename T>
 int Engine<T>::set_seg_len(int rows) {
   if (rows < 1) return LE2D_EINVAL;
   seg_len_ = rows;
+  seg_set_ = true;
+  return LE2D_OK;
+}
+
+template <typename T>
+int Engine<T>::set_depth(int depth) {
+  if (depth < 1 || depth > 2) return LE2D_EINVAL;
+  depth_set_ = depth;
+  return LE2D_OK;
+}
+
+// ---------------------------------------------------------------- batched autotuner
+
+namespace {
+std::mutex g_bt_mu;
+std::map<std::pair<int, int>, BatchTuned> g_bt;
+
+int ceil_log2(int n) {
+  int k = 0;
+  while ((1 << k) < n) ++k;
+  return k;
+}
+}  // namespace
+
+bool batch_tuned(int nx, int ny, BatchTuned* out) {
+  std::lock_guard<std::mutex> lk(g_bt_mu);
+  auto it = g_bt.find({ceil_log2(nx), ceil_log2(ny)});
+  if (it == g_bt.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+void batch_tune_reset() {
+  std::lock_guard<std::mutex> lk(g_bt_mu);
+  g_bt.clear();
+}
+
+// Times the batched kernel on copies of a scratch nx x ny problem (a disk of radius
+// min(nx,ny)/4 on a zero field, c1 = 2, c2 = 1, rho = 1, Courant number 0.5; enough copies
+// for ~24 M nodes, at most 256) for every tile height and steps per work item, and keeps
+// the fastest for the size class.
+template <typename T>
+int batch_autotune(int nx, int ny, BatchTuned* best) {
+  le2d_problem p;
+  std::memset(&p, 0, sizeof(p));
+  p.nx = nx;
+  p.ny = ny;
+  p.hx = p.hy = 1;
+  p.dt = (real)0.25;
+  p.c1 = 2;
+  p.c2 = 1;
+  p.rho = 1;
+  p.stype = ST_AOS;
+  p.receiver_row = -1;
+  p.receiver_every = 1;
+  const double nodes = (double)nx * ny;
+  const int copies = (int)std::max(1.0, std::min(256.0, std::ceil(24e6 / nodes)));
+  int steps = (int)std::min(512.0, std::max(8.0, 4e9 / (copies * nodes)));
+  steps += steps & 1;
+  p.steps = steps;
+  const T disk[4] = {(T)(nx / 2), (T)(ny / 2), (T)(std::min(nx, ny) / 4), (T)1};
+  const size_t budget = Engine<T>::footprint(p) * copies + ((size_t)64 << 20);
+  const int segs[] = {16, 32, 64, 128, 256};
+  best->nu_s = -1.0;
+  bool warm = false;
+  for (int d = 1; d <= batch_depth<T>(); ++d) {
+    for (int seg : segs) {
+      if (seg > ny && seg != segs[0]) continue;
+      for (int rep = 0; rep < (warm ? 1 : 2); ++rep) {  // the first trial runs twice (warm-up)
+        Engine<T> e(budget);
+        if (!e.ok()) return LE2D_ENOMEM;
+        e.set_seg_len(seg);
+        e.set_depth(d);
+        for (int k = 0; k < copies; ++k) {
+          const int id = e.add(p, nullptr, 1, disk);
+          if (id < 0) return -id;
+        }
+        float ms = 0.0f;
+        const int rc = e.run_all(steps, &ms);
+        if (rc) return rc;
+        const double nus = copies * nodes * steps / (ms * 1e-3);
+        if (rep == (warm ? 0 : 1) && nus > best->nu_s) {
+          best->nu_s = nus;
+          best->seg_len = seg;
+          best->depth = d;
+        }
+      }
+      warm = true;
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_bt_mu);
+  g_bt[{ceil_log2(nx), ceil_log2(ny)}] = *best;
   return LE2D_OK;
 }
 
@@ -161,14 +255,28 @@ int Engine<T>::add(const le2d_problem& p, const T* init, int ndisks, const T* di
   in.buf[0] = reinterpret_cast<T*>(arena_->base() + in.state_off);
   in.buf[1] = in.buf[0] + 5 * in.plane;
   in.c = problem_consts<T>(p);
+  // Tile height and steps per work item: explicit (autotuner trials), else the autotuner's
+  // table for the size class (LE2D_AUTOTUNE=1 tunes a class on first use), else defaults.
+  int seg = seg_len_, depth = batch_depth<T>();
+  if (!seg_set_ && !depth_set_) {
+    BatchTuned bt;
+    bool have = batch_tuned(p.nx, p.ny, &bt);
+    const char* a = getenv("LE2D_AUTOTUNE");
+    if (!have && a && atoi(a) != 0) have = batch_autotune<T>(p.nx, p.ny, &bt) == LE2D_OK;
+    if (have) {
+      seg = bt.seg_len;
+      depth = bt.depth;
+    }
+  }
+  if (depth_set_) depth = std::min(depth_set_, batch_depth<T>());
   // le_step_soa's far end is not a clamp: its instances advance one step per work item
-  in.depth = p.stype == ST_AOS ? batch_depth<T>() : 1;
+  in.depth = p.stype == ST_AOS ? depth : 1;
   // one- and two-step tiles have the same strips at the two-step kernel's 4 columns per
   // lane (one halo lane per side for either)
   static_assert(strip_cols(4) == strip_cols2(4), "strip widths of one and two steps");
   const int out = strip_cols(batch_lanes<T>());
   in.nstrips = (p.nx + out - 1) / out;
-  in.seg_len = std::min(seg_len_, p.ny);
+  in.seg_len = std::min(seg, p.ny);
   in.nsegs = (p.ny + in.seg_len - 1) / in.seg_len;
   in.live = true;
   cudaError_t e = cudaMemsetAsync(in.buf[0], 0, sbytes, stream_);
@@ -491,6 +599,7 @@ void Engine<T>::release(int id) {
 
 template class Engine<real>;
 template StepConsts<real> problem_consts<real>(const le2d_problem&);
+template int batch_autotune<real>(int, int, BatchTuned*);
 
 }  // namespace le2d
 
@@ -549,6 +658,29 @@ int le2d_batch_receivers(le2d_batch* b, int id, real* out, int* nsamples) {
 
 int le2d_batch_diagnostics(le2d_batch* b, int id, le2d_diag_t* out) {
   return b ? b->eng->diagnostics(id, out) : LE2D_EINVAL;
+}
+
+int le2d_batch_autotune(int nx, int ny, int* out, double* nu_per_s) {
+  if (nx < 3 || ny < 3) return LE2D_EINVAL;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return LE2D_ENODEV;
+  }
+  le2d::BatchTuned t;
+  const int rc = le2d::batch_autotune<real>(nx, ny, &t);
+  if (rc) return rc;
+  if (out) {
+    out[0] = t.seg_len;
+    out[1] = t.depth;
+  }
+  if (nu_per_s) *nu_per_s = t.nu_s;
+  return LE2D_OK;
+}
+
+int le2d_batch_autotune_reset(void) {
+  le2d::batch_tune_reset();
+  return LE2D_OK;
 }
 
 int le2d_batch_set_wait_limit(le2d_batch* b, unsigned long long ns) {

@@ -76,7 +76,11 @@ class Engine {
   int count() const { return (int)insts_.size(); }
   const Inst& inst(int id) const { return insts_[id]; }
   void set_wait_ns(unsigned long long ns) { wait_ns_ = ns; }
+  // Tile height and steps per work item for instances added afterwards (the autotuner's
+  // trials); otherwise they come from the autotuner's table for the instance's size class,
+  // or the defaults (64 rows, batch_depth<T>()).
   int set_seg_len(int rows);
+  int set_depth(int depth);
   size_t arena_used() const { return arena_ ? arena_->used() : 0; }
   size_t arena_capacity() const { return arena_ ? arena_->capacity() : 0; }
   long long node_updates() const { return node_updates_; }
@@ -104,6 +108,8 @@ class Engine {
   unsigned long long wait_ns_ = 2000000000ULL;
   int stall_tile_ = -1;  // test hook from LE2D_TEST_STALL_TILE (see launch_batch)
   int seg_len_ = 64;
+  bool seg_set_ = false;
+  int depth_set_ = 0;
   int resident_blocks_ = 0;
   long long node_updates_ = 0;
   // device scratch of the persistent launches (work lists, counters)
@@ -120,5 +126,16 @@ class Engine {
 // Constants of one problem's step (same derivation as the single-solve path).
 template <typename T>
 StepConsts<T> problem_consts(const le2d_problem& p);
+
+// Batched-path autotuner (per size class: nx, ny rounded up to powers of two): the fastest
+// tile height and steps per work item measured on copies of a scratch problem.
+struct BatchTuned {
+  int seg_len = 0, depth = 0;
+  double nu_s = 0.0;
+};
+template <typename T>
+int batch_autotune(int nx, int ny, BatchTuned* out);
+bool batch_tuned(int nx, int ny, BatchTuned* out);  // table lookup
+void batch_tune_reset();
 
 }  // namespace le2d
