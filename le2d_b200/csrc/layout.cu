@@ -67,6 +67,25 @@ __global__ void set_ball_kernel(T* __restrict__ soa, int nx, int ny, long long p
   }
 }
 
+// |v| = sqrt(vx^2 + vy^2) as the reference's VTK writer stores it (simple/le_core.c:99-111,
+// :150-165): the squares and their sum rounded one at a time in T, the square root in
+// double (correctly rounded, as the host's sqrt), rounded to float, stored big-endian;
+// nodes in the order j outer, i inner.
+template <typename T>
+__global__ void vtk_speed_kernel(const T* __restrict__ soa, int nx, int ny, long long pitch,
+                                 long long plane, unsigned* __restrict__ out) {
+  const long long n = (long long)nx * ny;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const long long j = q / nx, i = q - j * nx;
+    const T* s = soa + j * pitch + i;
+    const T vx = s[VX * plane], vy = s[VY * plane];
+    const T s2 = add_rn(mul_rn(vx, vx), mul_rn(vy, vy));
+    const float v = (float)sqrt((double)s2);
+    out[q] = __byte_perm(__float_as_uint(v), 0, 0x0123);
+  }
+}
+
 inline int grid_for(long long n) {
   long long b = (n + 255) / 256;
   if (b > 148LL * 16) b = 148LL * 16;
@@ -97,13 +116,22 @@ cudaError_t launch_set_ball(T* soa, int nx, int ny, long long pitch, long long p
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_vtk_speed(const T* soa, int nx, int ny, long long pitch, long long plane,
+                             unsigned* out, cudaStream_t s) {
+  vtk_speed_kernel<T><<<grid_for((long long)nx * ny), 256, 0, s>>>(soa, nx, ny, pitch, plane, out);
+  return cudaGetLastError();
+}
+
 #define LE2D_INST(T)                                                                             \
   template cudaError_t launch_pack<T>(const T*, T*, int, int, long long, long long, int,         \
                                       cudaStream_t);                                             \
   template cudaError_t launch_unpack<T>(const T*, T*, int, int, long long, long long, int,       \
                                         cudaStream_t);                                           \
   template cudaError_t launch_set_ball<T>(T*, int, int, long long, long long, T, T, T, T, T, T, \
-                                          cudaStream_t);
+                                          cudaStream_t);                                           \
+  template cudaError_t launch_vtk_speed<T>(const T*, int, int, long long, long long, unsigned*,  \
+                                           cudaStream_t);
 LE2D_INST(float)
 LE2D_INST(double)
 #undef LE2D_INST

@@ -613,12 +613,50 @@ void le_set_ball(le_task* t, const le_vec2 c, const real r, const real s) {
 }
 
 // simple/le_core.c:130-169 with write_float :99-111: header, then |v| as big-endian float32.
+// When the device holds the newest state, |v| is formed there (the same bytes, see
+// launch_vtk_speed) and only those 4 bytes per node cross to the host, not the 20 of the
+// full state; task->grid is then left as it is (le2d_sync_host refreshes it).
 int le_save_task(le_task* t, const char* file) {
   DevTask* d = lookup(t);
-  if (d && ensure_host_current(d, t)) return 1;
+  const long long n = (long long)t->n.x * t->n.y;
+  unsigned char* body = (unsigned char*)malloc(4 * (size_t)(n > 0 ? n : 1));
+  if (!body) {
+    fprintf(stderr, "le2d: le_save_task: host allocation failed\n");
+    return 1;
+  }
+  if (d && d->has_device && !d->host_newer) {
+    unsigned* scratch = reinterpret_cast<unsigned*>(d->buf[d->cur ^ 1]);  // the idle buffer
+    cudaError_t e = le2d::launch_vtk_speed<T>(d->buf[d->cur], d->nx, d->ny, d->pitch, d->plane,
+                                              scratch, d->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(body, scratch, 4 * (size_t)n, cudaMemcpyDeviceToHost, d->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+    if (e != cudaSuccess || check_pairs(d) != LE2D_OK) {
+      if (e != cudaSuccess) record(d, LE2D_ECUDA, "le_save_task", e);
+      free(body);
+      return 1;
+    }
+  } else {
+    if (d && ensure_host_current(d, t)) {
+      free(body);
+      return 1;
+    }
+    for (long long q = 0; q < n; q++) {
+      const real vx = t->stype == ST_AOS ? t->grid[q * 5 + 0] : t->grid[q];
+      const real vy = t->stype == ST_AOS ? t->grid[q * 5 + 1] : t->grid[n + q];
+      const float v = sqrt(vx * vx + vy * vy);
+      unsigned char b[4];
+      memcpy(b, &v, 4);
+      body[4 * q + 0] = b[3];
+      body[4 * q + 1] = b[2];
+      body[4 * q + 2] = b[1];
+      body[4 * q + 3] = b[0];
+    }
+  }
   FILE* fp = fopen(file, "w");
   if (!fp) {
     perror("Failed to open file");
+    free(body);
     return 1;
   }
   fprintf(fp, "# vtk DataFile Version 3.0\n");
@@ -631,25 +669,8 @@ int le_save_task(le_task* t, const char* file) {
   fprintf(fp, "POINT_DATA %d\n", t->n.x * t->n.y);
   fprintf(fp, "SCALARS v float 1\n");
   fprintf(fp, "LOOKUP_TABLE v_table\n");
-  const long long plane = (long long)t->n.x * t->n.y;
-  const int nx = t->n.x;
-  unsigned char* row = (unsigned char*)malloc(4 * (size_t)nx);
-  for (int j = 0; j < t->n.y && row; j++) {
-    for (int i = 0; i < nx; i++) {
-      const long long q = i + (long long)j * nx;
-      const real vx = t->stype == ST_AOS ? t->grid[q * 5 + 0] : t->grid[q];
-      const real vy = t->stype == ST_AOS ? t->grid[q * 5 + 1] : t->grid[plane + q];
-      const float v = sqrt(vx * vx + vy * vy);
-      unsigned char b[4];
-      memcpy(b, &v, 4);
-      row[4 * i + 0] = b[3];
-      row[4 * i + 1] = b[2];
-      row[4 * i + 2] = b[1];
-      row[4 * i + 3] = b[0];
-    }
-    fwrite(row, 1, 4 * (size_t)nx, fp);
-  }
-  free(row);
+  fwrite(body, 1, 4 * (size_t)n, fp);
+  free(body);
   fclose(fp);
   return 0;
 }

@@ -75,6 +75,12 @@ template <typename T>
 cudaError_t launch_unpack(const T* soa, T* raw, int nx, int ny, long long pitch,
                           long long plane, int aos, cudaStream_t s);
 
+// The VTK writer's scalar: |v| of every node as a big-endian float32, rows j outer
+// (out: nx*ny words), the same bytes as the host writer computes.
+template <typename T>
+cudaError_t launch_vtk_speed(const T* soa, int nx, int ny, long long pitch, long long plane,
+                             unsigned* out, cudaStream_t s);
+
 // le_set_ball on the device state (same arithmetic as the host loop).
 template <typename T>
 cudaError_t launch_set_ball(T* soa, int nx, int ny, long long pitch, long long plane, T hx, T hy,

@@ -375,3 +375,35 @@ def test_pair_bounded_wait_gives_up(libs, monkeypatch):
         finally:
             lib.le_free_task(t)
     assert outs[0].tobytes() == outs[1].tobytes()
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_save_task_from_device_bytes(libs, prec, tmp_path):
+    """le_save_task forms |v| on the device (4 bytes per node cross to the host): the file is
+    byte-identical to the reference writer's -- the golden file of the reference, and the
+    oracle's writer on stepped states in both layouts."""
+    lib = libs[prec]
+    c = cases()["ball_64x48"]
+    t = make_task(lib, c)
+    try:
+        assert lib.upload(t, arrays(prec)["ball_64x48__out"].copy()) == 0
+        path = tmp_path / "golden.vtk"
+        assert lib.le_save_task(t, str(path)) == 0
+        assert path.read_bytes() == arrays(prec)["ball_64x48__vtk"].tobytes()
+    finally:
+        lib.le_free_task(t)
+    for stype in (ST_AOS, ST_SOA):
+        p, g0, steps = _medium(prec, stype, 131, 77, 9)
+        t = make_task(lib, p)
+        try:
+            assert lib.upload(t, g0.copy()) == 0
+            assert lib.step_n(t, steps) == 0
+            path = tmp_path / f"dev{stype}.vtk"
+            assert lib.le_save_task(t, str(path)) == 0
+            state = np.zeros_like(g0)
+            assert lib.download(t, state) == 0
+        finally:
+            lib.le_free_task(t)
+        ref = tmp_path / f"oracle{stype}.vtk"
+        assert Oracle(prec).save_vtk(state, p["nx"], p["ny"], p["hx"], p["hy"], stype, str(ref)) == 0
+        assert path.read_bytes() == ref.read_bytes(), stype
