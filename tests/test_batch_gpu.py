@@ -152,3 +152,28 @@ def test_batch_bounded_wait_gives_up(libs, monkeypatch):
         assert b.run()[0] == 0
         want, _ = solve_alone(lib, p, ST_AOS)
         assert b.fields(i).tobytes() == want.tobytes()
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_batch_odd_windows_and_receivers(libs, prec):
+    """Odd window lengths (a two-step instance then ends a window with a one-step item) and
+    samples every 3 steps (taken after the first step of a two-step item on the producer
+    warp, after the second on the consumer, and after one-step items): fields and receiver
+    lines bitwise equal to the instances solved alone."""
+    lib = libs[prec]
+    rng = np.random.default_rng(9)
+    probs = small_set(24, 4, 20, 260, 17, 41)
+    stypes = [ST_AOS, ST_AOS, ST_SOA, ST_AOS]
+    with capi.Batch(lib, 1 << 30) as b:
+        inits, ids = [], []
+        for p, st in zip(probs, stypes):
+            g = rng.uniform(-0.1, 0.1, 5 * p.nx * p.ny).astype(lib.dtype)
+            inits.append(g)
+            ids.append(b.add(b.problem(p, st, receiver_row=p.ny // 3, receiver_every=3), init=g))
+        assert b.run(window_steps=7)[0] == 0
+        for i, p, st, g in zip(ids, probs, stypes, inits):
+            want, samples = solve_alone(lib, p, st, init=g, sample_row=p.ny // 3, every=3)
+            assert b.fields(i).tobytes() == want.tobytes(), (i, st)
+            rec = b.receivers(i)
+            assert rec.shape == (p.steps // 3, 2, p.nx)
+            assert rec.tobytes() == samples.astype(lib.dtype).tobytes(), (i, st)
