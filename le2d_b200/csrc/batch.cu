@@ -22,9 +22,10 @@
 // FP32 items advance two steps (temporal blocking) on a producer / consumer warp pair
 // (march_pair.cuh): the producer claims the item, passes its index to the consumer through
 // the pair's queue, waits for the item's dependencies, reads the state and runs the first
-// step; the consumer runs the second step on the rows it is handed, writes them and
-// publishes the tile.  The last item of an odd step count, and every item of an
-// le_step_soa instance, advances one step on the producer alone, which then publishes.
+// step; the consumer runs the second step on the rows it is handed, writes them, records
+// receiver samples and publishes the tile.  The last item of an odd step count, and every
+// item of an le_step_soa instance, advances one step: the consumer writes the producer's
+// rows as they are.
 // A producer may claim its next item while its consumer still finishes the last one: all
 // rows of that item are already in the queue, so the consumer finishes without it.
 #include <type_traits>
@@ -163,7 +164,6 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
     const BatchTile bt = tiles[q - step_items[r]];
     const BatchInst<T>& I = insts[bt.inst];
     const int nadv = min(I.depth, I.steps - r * I.depth);  // steps this item advances
-    if (!producer && nadv == 1) continue;  // the producer advances one-step items alone
     if (producer && r > 0 &&
         !wait_neighbours(done, I.tile_base, I.nstrips, I.nsegs, bt.seg, bt.strip, r, ctl, wait_ns))
       break;
@@ -171,18 +171,23 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
     const march::GridRef<T> g{I.buf[par], I.buf[par ^ 1], I.nx, I.ny, I.pitch, I.plane, I.far_rot};
     const int y0 = bt.seg * I.seg_len;
     const int y1 = min(y0 + I.seg_len, I.ny);
-    // absolute step count the rows this warp writes (or hands over) complete
-    const long long after = I.abs_step0 + (long long)r * I.depth + (producer ? 1 : 2);
-    march::RowTap<T> tap{nullptr, -1};
-    if (I.trace != nullptr && after % I.trace_every == 0)
-      tap = march::RowTap<T>{I.trace + (after / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
-    const bool ok =
-        producer ? march::pair_produce<T, V, kNpf, true, true>(g, I.c, bt.strip, y0, y1, smem, bars,
-                                                               wait_ns, status, u, nadv == 1, tap)
-                 : march::pair_consume<T, V, kNpf, true>(g, I.c, bt.strip, y0, y1, smem, bars,
-                                                         wait_ns, status, u, tap);
+    bool ok;
+    if (producer) {
+      ok = march::pair_produce<T, V, kNpf, true>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
+                                                 u, nadv == 1);
+    } else {
+      // receiver samples after the item's first and (two-step items) second step
+      const long long before = I.abs_step0 + (long long)r * I.depth;
+      march::RowTap<T> tap_a{nullptr, -1}, tap_b{nullptr, -1};
+      if (I.trace != nullptr && (before + 1) % I.trace_every == 0)
+        tap_a = march::RowTap<T>{I.trace + ((before + 1) / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
+      if (I.trace != nullptr && nadv == 2 && (before + 2) % I.trace_every == 0)
+        tap_b = march::RowTap<T>{I.trace + ((before + 2) / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
+      ok = march::pair_consume<T, V, kNpf, true>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
+                                                 u, nadv == 1, tap_a, tap_b);
+    }
     if (!ok) break;
-    if (producer == (nadv == 1)) {  // the warp that wrote the tile's new state publishes it
+    if (!producer) {  // the consumer wrote the tile's new state and publishes it
       __syncwarp();
       const int tile_id = I.tile_base + bt.seg * I.nstrips + bt.strip;
       if (lane == 0 && !(r == 0 && tile_id == stall_plus1 - 1)) {

@@ -91,8 +91,10 @@ __host__ __device__ constexpr int pair_smem_bytes() {
 }
 
 // How many rows of step B's stencil step-A row ka stands for (tile rows [y0, y1)):
-// step B reads rows [y0-2, y1+2) clamped to [0, ny).
-__device__ __forceinline__ int row_uses(int ka, int y0, int y1, int ny) {
+// step B reads rows [y0-2, y1+2) clamped to [0, ny).  A one-step tile hands over its own
+// rows [y0, y1) only, once each.
+__device__ __forceinline__ int row_uses(int ka, int y0, int y1, int ny, bool one_step = false) {
+  if (one_step) return ka >= y0 && ka < y1 ? 1 : 0;
   int reps = ka < 0 || ka >= ny ? 0 : 1;
   if (ka == 0 && y0 < 2) reps += 2 - y0;
   if (ka == ny - 1 && y1 + 2 > ny) reps += y1 + 2 - ny;
@@ -115,16 +117,15 @@ __device__ __forceinline__ void tap_row(const RowTap<T>& tap, long long pitch, i
 }
 
 // Producer warp: step A of strip `strip`, rows [y0, y1) of the tile, handing its rows to
-// the consumer; `u` counts the queue's handoffs (it continues across tiles).  With
-// one_step the warp instead writes step A's rows [y0, y1) to g.dst itself (a tile that
-// advances one step: an odd last step, or le_step_soa's far end, which g.far_rot selects).
-// `tap` (TAP): receiver row of step A's rows.  Returns false if a wait gave up.
-template <typename T, int V, int NPF, bool COHERENT, bool TAP>
+// the consumer; `u` counts the queue's handoffs (it continues across tiles).  A one_step
+// tile (an odd last step, or le_step_soa's far end, which g.far_rot selects) hands over
+// step A's rows [y0, y1) only, which the consumer writes.  Returns false if a wait gave up.
+template <typename T, int V, int NPF, bool COHERENT>
 __device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepConsts<T>& c, int strip,
                                              int y0, int y1, T* smem_pair,
                                              unsigned long long* bars,
                                              unsigned long long wait_ns, int* status, unsigned& u,
-                                             bool one_step, const RowTap<T>& tap) {
+                                             bool one_step) {
   using VT = typename Vec<T, V>::type;
   static_assert(NPF >= 2, "the input ring needs at least the current and the next row");
   static_assert(!COHERENT || V * sizeof(T) == 16, "coherent loads need 16-byte (L2-only) copies");
@@ -141,7 +142,6 @@ __device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepCons
   const int xs = strip * kOut - H2 * V;
   const int col0 = xs + lane * V;
   const bool interior = xs >= 0 && xs + kIn <= g.nx;
-  const bool writer = lane >= H2 && lane < 32 - H2 && col0 < g.nx;
   const int mend = one_step ? y1 + 2 : y1 + 4;  // one step needs the raw rows up to y1+1 only
 
   YPipe<T, V> ya;
@@ -172,21 +172,9 @@ __device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepCons
     sweep_x_lane<T, V>(f, c.x);
     ring_left(ya, f, a_ring, aslot, c.y);
     const int ka = m - 2;  // step-A row completed now
-    if (one_step) {
-      if (m >= y0 + 2) {  // ka in [y0, y1)
-        T ga[NF][V];
-        ring_output(ya, ga, a_ring, aslot, c.y);
-        if (writer) {
-          T* out = g.dst + (long long)ka * g.pitch + col0;
-#pragma unroll
-          for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(out + k * g.plane) = pack(ga[k]);
-          if (TAP && ka == tap.row) tap_row<T, V>(tap, g.pitch, col0, ga);
-        }
-      }
-    } else if (m >= y0 && row_uses(ka, y0, y1, g.ny) > 0) {
+    if (m >= y0 && row_uses(ka, y0, y1, g.ny, one_step) > 0) {
       T ga[NF][V];
       ring_output(ya, ga, a_ring, aslot, c.y);
-      if (TAP && ka == tap.row && ka >= y0 && ka < y1 && writer) tap_row<T, V>(tap, g.pitch, col0, ga);
       if (!interior) clamp_columns<T, V>(ga, xs, col0, g.nx);
       const int hs = (int)(u % kHand);
       const unsigned use = u / kHand;
@@ -209,13 +197,16 @@ __device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepCons
 }
 
 // Consumer warp: step B of the same tile, writing rows [y0, y1) to g.dst; `u` as for the
-// producer, `tap` (TAP): receiver row of step B's rows.  Returns false if a wait gave up.
+// producer.  A one_step tile's handed rows are step A's rows [y0, y1), written as they
+// are.  TAP: receiver rows -- tap_a of the rows after step A (taken from the handed rows),
+// tap_b of the rows after step B.  Returns false if a wait gave up.
 template <typename T, int V, int NPF, bool TAP>
 __device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepConsts<T>& c, int strip,
                                              int y0, int y1, T* smem_pair,
                                              unsigned long long* bars,
                                              unsigned long long wait_ns, int* status, unsigned& u,
-                                             const RowTap<T>& tap) {
+                                             bool one_step, const RowTap<T>& tap_a,
+                                             const RowTap<T>& tap_b) {
   using VT = typename Vec<T, V>::type;
   constexpr int H2 = halo_lanes2(V);
   constexpr int kIn = 32 * V;
@@ -237,11 +228,30 @@ __device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepCons
   int bslot = 0;
   int bin = y0 - 2;  // step-B row index of the next row fed to step B
   for (int ka = y0 - 2; ka < y1 + 2; ++ka) {
-    const int reps = row_uses(ka, y0, y1, g.ny);
+    const int reps = row_uses(ka, y0, y1, g.ny, one_step);
     if (reps == 0) continue;
     const int hs = (int)(u % kHand);
     if (!mbar_wait(full + hs, (u / kHand) & 1, wait_ns, status)) return false;
     const T* slot = hand + hs * kRow;
+    if (TAP && ka == tap_a.row && ka >= y0 && ka < y1 && writer) {
+      T fa[NF][V];
+#pragma unroll
+      for (int k = 0; k < NF; ++k) unpack(*reinterpret_cast<const VT*>(slot + k * kIn), fa[k]);
+      tap_row<T, V>(tap_a, g.pitch, col0, fa);
+    }
+    if (one_step) {  // step A's row ka in [y0, y1): written as handed over
+      T fa[NF][V];
+#pragma unroll
+      for (int k = 0; k < NF; ++k) unpack(*reinterpret_cast<const VT*>(slot + k * kIn), fa[k]);
+      mbar_arrive(empty + hs);
+      if (writer) {
+        T* out = g.dst + (long long)ka * g.pitch + col0;
+#pragma unroll
+        for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(out + k * g.plane) = pack(fa[k]);
+      }
+      ++u;
+      continue;
+    }
     for (int r = 0; r < reps; ++r) {  // the slot is read once per use, released after the last
       T fb[NF][V];
 #pragma unroll
@@ -257,7 +267,7 @@ __device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepCons
           T* out = g.dst + (long long)row * g.pitch + col0;
 #pragma unroll
           for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(out + k * g.plane) = pack(gb[k]);
-          if (TAP && row == tap.row) tap_row<T, V>(tap, g.pitch, col0, gb);
+          if (TAP && row == tap_b.row) tap_row<T, V>(tap_b, g.pitch, col0, gb);
         }
       }
       yb.right(c.y);

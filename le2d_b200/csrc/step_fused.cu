@@ -72,11 +72,11 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) fused_pair_kernel(const Fus
   unsigned u = 0;
   const march::RowTap<T> no_tap{nullptr, -1};
   if ((wib & 1) == 0)
-    march::pair_produce<T, V, NPF, false, false>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns,
-                                                 p.pair.status, u, false, no_tap);
+    march::pair_produce<T, V, NPF, false>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns,
+                                          p.pair.status, u, false);
   else
     march::pair_consume<T, V, NPF, false>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns,
-                                          p.pair.status, u, no_tap);
+                                          p.pair.status, u, false, no_tap, no_tap);
 }
 
 // Compiled variants: columns per lane V (one 16- or 8-byte access per field), the
