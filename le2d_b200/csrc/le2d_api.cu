@@ -56,6 +56,10 @@ struct DevTask {
   int method = LE2D_METHOD_FUSED;
   FusedPlan plan;
   FusedPlan plan1;  // depth-1 plan for single steps when `plan` has depth 2
+  // One le_step call held back under a two-step plan, so that the next call makes a
+  // two-step launch with it; queued by itself before anything else touches the state.
+  bool pending = false;
+  StepConsts<T> pending_c;
   long long steps = 0;
   double sim_time = 0.0;
   // CUDA graph of kGraphSteps steps starting from buffer graph_cur.
@@ -345,6 +349,22 @@ cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int meth
   return e;
 }
 
+// Queues a held-back le_step (one step) before the state is used otherwise.
+int flush_pending(DevTask* d) {
+  if (!d->pending) return LE2D_OK;
+  d->pending = false;
+  int done = 0;
+  const cudaError_t e = queue_step(d, d->pending_c, 0, d->method, &d->cur, 1, &done);
+  return e == cudaSuccess ? LE2D_OK : record(d, LE2D_ECUDA, "step kernel launch", e);
+}
+
+// lookup() for entry points that read, write or wait for the device state.
+DevTask* lookup_sync(const le_task* task) {
+  DevTask* d = lookup(task);
+  if (d) flush_pending(d);
+  return d;
+}
+
 int run_steps(le_task* task, int nsteps, bool soa_entry, float* ms) {
   DevTask* d = lookup(task);
   if (!d) {
@@ -360,6 +380,27 @@ int run_steps(le_task* task, int nsteps, bool soa_entry, float* ms) {
   if (rc) return rc;
   const StepConsts<T> c = make_consts(task);
   const int far_rot = soa_entry ? 1 : 0;
+  // One le_step call under a two-step plan: held back, and launched as two steps together
+  // with the next call (same constants); any other use of the state queues it first.
+  if (nsteps == 1 && !soa_entry && !ms && d->method == LE2D_METHOD_FUSED && d->plan.depth == 2) {
+    if (d->pending && same_consts(d->pending_c, c)) {
+      d->pending = false;
+      int done = 0;
+      const cudaError_t e1 = queue_step(d, c, 0, d->method, &d->cur, 2, &done);
+      if (e1 != cudaSuccess) return record(d, LE2D_ECUDA, "step kernel launch", e1);
+    } else {
+      rc = flush_pending(d);
+      if (rc) return rc;
+      d->pending = true;
+      d->pending_c = c;
+    }
+    d->sim_time += (double)task->dt;
+    d->steps += 1;
+    d->dev_newer = true;
+    return LE2D_OK;
+  }
+  rc = flush_pending(d);
+  if (rc) return rc;
   cudaError_t e = cudaSuccess;
   if (ms) {
     e = cudaEventRecord(d->ev[0], d->stream);
@@ -592,7 +633,7 @@ void le_free_task(le_task* task) {
 }
 
 void le_set_ball(le_task* t, const le_vec2 c, const real r, const real s) {
-  DevTask* d = lookup(t);
+  DevTask* d = lookup_sync(t);
   if (t->stype != ST_AOS && t->stype != ST_SOA) {
     record(d, LE2D_EINVAL, "le_set_ball: unknown stype");
     return;
@@ -617,7 +658,7 @@ void le_set_ball(le_task* t, const le_vec2 c, const real r, const real s) {
 // launch_vtk_speed) and only those 4 bytes per node cross to the host, not the 20 of the
 // full state; task->grid is then left as it is (le2d_sync_host refreshes it).
 int le_save_task(le_task* t, const char* file) {
-  DevTask* d = lookup(t);
+  DevTask* d = lookup_sync(t);
   const long long n = (long long)t->n.x * t->n.y;
   unsigned char* body = (unsigned char*)malloc(4 * (size_t)(n > 0 ? n : 1));
   if (!body) {
@@ -701,13 +742,13 @@ int le2d_clear_error(le_task* task) {
 }
 
 int le2d_sync_host(le_task* task) {
-  DevTask* d = lookup(task);
+  DevTask* d = lookup_sync(task);
   if (!d) return LE2D_ENOTASK;
   return ensure_host_current(d, task);
 }
 
 int le2d_sync_device(le_task* task) {
-  DevTask* d = lookup(task);
+  DevTask* d = lookup_sync(task);
   if (!d) return LE2D_ENOTASK;
   d->host_newer = true;
   d->dev_newer = false;
@@ -715,7 +756,7 @@ int le2d_sync_device(le_task* task) {
 }
 
 int le2d_upload(le_task* task, const real* src) {
-  DevTask* d = lookup(task);
+  DevTask* d = lookup_sync(task);
   if (!d) return LE2D_ENOTASK;
   if (!src) return record(d, LE2D_EINVAL, "le2d_upload: NULL source");
   if (!d->has_device) return record(d, LE2D_ENODEV, "le2d_upload");
@@ -727,7 +768,7 @@ int le2d_upload(le_task* task, const real* src) {
 }
 
 int le2d_download(le_task* task, real* dst) {
-  DevTask* d = lookup(task);
+  DevTask* d = lookup_sync(task);
   if (!d) return LE2D_ENOTASK;
   if (!dst) return record(d, LE2D_EINVAL, "le2d_download: NULL destination");
   if (d->host_newer) {
@@ -752,7 +793,7 @@ void le2d_host_free(void* p) {
 }
 
 int le2d_wait(le_task* task) {
-  DevTask* d = lookup(task);
+  DevTask* d = lookup_sync(task);
   if (!d) return LE2D_ENOTASK;
   if (!d->has_device) return LE2D_OK;
   cudaError_t e = cudaStreamSynchronize(d->stream);
@@ -760,7 +801,7 @@ int le2d_wait(le_task* task) {
 }
 
 int le2d_set_method(le_task* task, int method) {
-  DevTask* d = lookup(task);
+  DevTask* d = lookup_sync(task);
   if (!d) return LE2D_ENOTASK;
   if (method != LE2D_METHOD_FUSED && method != LE2D_METHOD_SPLIT) return LE2D_EINVAL;
   d->method = method;
@@ -768,7 +809,7 @@ int le2d_set_method(le_task* task, int method) {
 }
 
 int le2d_set_variant(le_task* task, int variant, int seg_len) {
-  DevTask* d = lookup(task);
+  DevTask* d = lookup_sync(task);
   if (!d) return LE2D_ENOTASK;
   if (variant < -1 || variant >= le2d::fused_variant_count<T>() || seg_len < 0) return LE2D_EINVAL;
   if (!d->has_device) return LE2D_ENODEV;
@@ -835,7 +876,7 @@ int le2d_sim_time(const le_task* task, double* t, long long* steps) {
 }
 
 int le2d_diagnostics(le_task* task, le2d_diag_t* out) {
-  DevTask* d = lookup(task);
+  DevTask* d = lookup_sync(task);
   if (!d) return LE2D_ENOTASK;
   if (!out) return LE2D_EINVAL;
   int rc = ensure_device_current(d, task);

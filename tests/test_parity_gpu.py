@@ -407,3 +407,53 @@ def test_save_task_from_device_bytes(libs, prec, tmp_path):
         ref = tmp_path / f"oracle{stype}.vtk"
         assert Oracle(prec).save_vtk(state, p["nx"], p["ny"], p["hx"], p["hy"], stype, str(ref)) == 0
         assert path.read_bytes() == ref.read_bytes(), stype
+
+
+def test_per_call_steps_pair_up(libs):
+    """Under a two-step plan, consecutive le_step calls run as two-step launches; a step held
+    back is queued by itself before anything else touches the state (set_ball, diagnostics,
+    download, save, step_n), and a changed dt is not paired with the previous call's.  The
+    results are bitwise those of a one-step plan through the same call sequence."""
+    lib = libs["f"]
+    vs = variants(lib)
+    two = [v for v in vs if vs[v] == 2][-1]
+    c = dict(nx=150, ny=97, hx=1.0, hy=1.0, c1=2.0, c2=1.0, rho=1.0, dt=0.25, stype=ST_AOS)
+
+    def sequence(variant):
+        t = make_task(lib, c)
+        log = []
+        try:
+            assert lib.set_variant(t, variant, 0) == 0
+            lib.le_set_ball(t, (75.0, 48.0), 20.0, 1.0)
+            for _ in range(3):
+                lib.le_step(t)
+            lib.le_set_ball(t, (30.0, 30.0), 8.0, -0.5)
+            lib.le_step(t)
+            rc, dg = lib.diagnostics(t)
+            assert rc == 0
+            log.append(dg["energy"])
+            for _ in range(2):
+                lib.le_step(t)
+            t.dt = 0.2  # the next call's constants differ from the held-back one's
+            lib.le_step(t)
+            lib.le_step(t)
+            lib.le_step(t)
+            assert lib.step_n(t, 5) == 0
+            lib.le_step(t)
+            g = np.zeros(5 * c["nx"] * c["ny"], lib.dtype)
+            assert lib.download(t, g) == 0
+            log.append(lib.sim_time(t))
+            lib.le_step(t)
+            assert lib.sync_host(t) == 0
+            assert lib.last_error(t) == 0
+            return g, lib.grid_view(t).copy(), log
+        finally:
+            lib.le_free_task(t)
+
+    a = sequence(two)
+    b = sequence(2)
+    assert a[0].tobytes() == b[0].tobytes()
+    assert a[1].tobytes() == b[1].tobytes()
+    # the FP64 energy is a sum in atomic order (equal to ~1e-15), the simulated time exact
+    assert abs(a[2][0] - b[2][0]) <= 1e-12 * abs(b[2][0])
+    assert a[2][1] == b[2][1]
