@@ -68,8 +68,11 @@ __device__ __forceinline__ float ratio(float a, float b) {
 // refined by two Newton steps y <- y + y (1 - b y) (each doubles the correct bits), and the
 // quotient q = a y by one correction with its FMA residual, q + (a - b q) y (Markstein's
 // final step): within an ulp of the IEEE quotient, at about half the instructions of the
-// full division sequence.  For b = +-0 the estimate is +-inf and for b = +-inf it is 0; in
-// both cases a * y0 already equals a / b (+-inf / NaN, or 0), so that product is returned.
+// full division sequence.  Outside 2^-1022 <= |b| < 2^1022 (b = +-0, denormal, huge,
+// +-inf, NaN) the iteration breaks down, but the estimate is +-inf, 0 or NaN there and
+// a * y0 is the quotient's limit the limiter needs (+-inf / NaN for b = 0, 0 for huge or
+// infinite b); the choice is a select, not a branch (a branch per ratio costs more than the
+// division).
 __device__ __forceinline__ double ratio(double a, double b) {
   double y0;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(b));
@@ -77,7 +80,9 @@ __device__ __forceinline__ double ratio(double a, double b) {
   y = fma(y, fma(-b, y, 1.0), y);
   const double q = a * y;
   const double r = fma(fma(-b, q, a), y, q);
-  return (y0 == 0.0 || isinf(y0)) ? a * y0 : r;
+  const double ab = fabs(b);
+  const bool normal = (ab >= 0x1p-1022) & (ab < 0x1p+1022);  // & : no short-circuit branch
+  return normal ? r : a * y0;
 }
 
 __device__ __forceinline__ float max3(float a, float b, float c) {
@@ -96,7 +101,10 @@ __device__ __forceinline__ float psi(float r, float kc) {
   return kc * fmaxf(__saturatef(r + r), fminf(2.0f, r));
 }
 __device__ __forceinline__ double psi(double r, double kc) {
-  return kc * max3(0.0, fmin(1.0, r + r), fmin(2.0, r));
+  // the two fmin results are never NaN, so the maxima are plain compare-selects
+  const double v = fmin(1.0, r + r), w = fmin(2.0, r);
+  const double m = v > w ? v : w;
+  return kc * (m > 0.0 ? m : 0.0);
 }
 
 // Differences of the four moving invariants across a face, formed from the differences

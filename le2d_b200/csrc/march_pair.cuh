@@ -19,7 +19,9 @@
 // Halos and boundaries as in march2.cuh: step A is valid on [xs+2, xs+32V-2), step B on
 // [xs+4, xs+32V-4); the producer overwrites step A's values outside [0, nx) with the edge
 // column's and hands row 0 / ny-1 over once and the consumer feeds it to step B once for
-// every row of its stencil it stands for (the same count both warps compute).
+// every row of its stencil it stands for (the same count both warps compute).  A one-step
+// tile (in the batched kernel: an odd last step, or le_step_soa's far end) hands over step
+// A's own rows [y0, y1), which the consumer writes as they are.
 #pragma once
 
 #include "march2.cuh"
