@@ -250,6 +250,14 @@ def cpu_reference_sample(p, budget_s=12.0):
     return out
 
 
+def single_config(p, parallelism: str) -> dict:
+    """The `config` of the single-solve workload (both arms)."""
+    return {"workload": f"single_8192: {p.nx}x{p.ny} grid, c1={p.c1}, c2={p.c2}, rho={p.rho}, "
+                        f"dt=0.5*h/c1, 8 seeded disks; one bench step = one solve of {p.steps} time steps",
+            "nx": p.nx, "ny": p.ny, "time_steps_per_solve": p.steps,
+            "l2": "state 1.34 GB (> 126 MB L2), no flush", "parallelism": parallelism}
+
+
 def run_reference_arm(args):
     world, rank, local = dist_setup()
     if rank != 0:
@@ -288,8 +296,8 @@ def run_reference_arm(args):
         "impl": "reference", "metric": "node-updates/s", "value": value, "unit": "node-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "single_8192 (one time step per bench step)", "nx": p.nx, "ny": p.ny,
-                   "parallelism": f"cpu{threads}"},
+        "config": {**single_config(p, f"host threads x{threads}"),
+                   "sample": "each bench step times one of the solve's time steps (per-step cost is constant)"},
         "cpu_baseline": {"value": value, "unit": "node-updates/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "node-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -632,10 +640,7 @@ def main():
         "metric": "node-updates/s", "value": value, "unit": "node-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": slow_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"single_8192: {p.nx}x{p.ny} grid, c1={p.c1}, c2={p.c2}, rho={p.rho}, "
-                               f"dt=0.5*h/c1, 8 seeded disks; one bench step = one solve of {p.steps} time steps",
-                   "nx": p.nx, "ny": p.ny, "time_steps_per_solve": p.steps,
-                   "l2": "state 1.34 GB (> 126 MB L2), no flush", "parallelism": f"independent solves x{world}"},
+        "config": single_config(p, f"independent solves x{world}"),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,
                      "traffic": traffic.get("bytes_per_launch") if traffic else None,
