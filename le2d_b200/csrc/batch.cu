@@ -65,13 +65,15 @@ __device__ __forceinline__ bool wait_neighbours(const int* done, int tile_base, 
   const int* p = done + tile_base + (watch ? s2 * nstrips + k2 : 0);
   const unsigned long long t0 = global_ns();
   unsigned ns = 32;
-  while (true) {
+  // gives up after wait_ns of global time over at least 1024 polls (a preempted block sees
+  // the clock run on without polling)
+  for (unsigned polls = 0;; ++polls) {
     const bool ready = !watch || ld_acquire(p) >= r;
     if (__all_sync(0xffffffffu, ready)) return true;
     int bail = 0;
     if (lane == 0) {
       bail = *reinterpret_cast<volatile int*>(&ctl->status) != 0;
-      if (!bail && global_ns() - t0 > wait_ns) {
+      if (!bail && polls >= 1024 && global_ns() - t0 > wait_ns) {
         atomicExch(&ctl->status, 1);
         bail = 1;
       }

@@ -13,8 +13,9 @@
 // `full`, the producer (from the second use of a slot on) for phase u / kHand - 1 of
 // `empty`.  Each lane reads back exactly the columns the same lane of the other warp wrote.
 //
-// Every wait is bounded by `wait_ns` of global time; a warp that gives up sets *status
-// and leaves, so its partner gives up too and the launch ends with the status set.
+// Every wait is bounded (wait_ns of global time over at least kMinPolls polls); a warp that
+// gives up sets *status and leaves, so its partner gives up too and the launch ends with
+// the status set.
 //
 // Halos and boundaries as in march2.cuh: step A is valid on [xs+2, xs+32V-2), step B on
 // [xs+4, xs+32V-4); the producer overwrites step A's values outside [0, nx) with the edge
@@ -60,19 +61,23 @@ __device__ __forceinline__ unsigned long long global_timer_ns() {
 }
 
 // Waits (all 32 lanes) for the completion of the phase of `bar` with parity `parity`.
-// Returns false, warp-uniformly, if it has not completed within wait_ns or the partner
-// has already given up (*status != 0).
+// Returns false, warp-uniformly, once it has waited more than wait_ns of global time over
+// at least kMinPolls polls, or as soon as the partner has given up (*status != 0).  Both
+// bounds must pass: a block that another context preempts sees the clock run on without
+// polling, and a poll that returns at once takes no time.
+constexpr unsigned kMinPolls = 1024;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity,
                                           unsigned long long wait_ns, int* status) {
   bool ok = mbar_test(bar, parity);
   if (__all_sync(0xffffffffu, ok)) return true;
   const unsigned long long t0 = global_timer_ns();
-  while (true) {
+  for (unsigned polls = 1;; ++polls) {
     if (!ok) ok = mbar_test(bar, parity);
     if (__all_sync(0xffffffffu, ok)) return true;
     int bail = 0;
     if ((threadIdx.x & 31) == 0)
-      bail = *reinterpret_cast<volatile int*>(status) != 0 || global_timer_ns() - t0 > wait_ns;
+      bail = *reinterpret_cast<volatile int*>(status) != 0 ||
+             (polls >= kMinPolls && global_timer_ns() - t0 > wait_ns);
     if (__shfl_sync(0xffffffffu, bail, 0)) {
       if ((threadIdx.x & 31) == 0) atomicExch(status, 1);
       return false;
