@@ -634,7 +634,8 @@ def main():
     # per node and launch
     alg_bytes = BYTES_PER_NU["f"] * p.nodes * depth
     achieved = alg_bytes / avg_launch_s / 1e9
-    kname = f"fused_step_kernel<float, V={plan['lanes']}, depth={depth}>"
+    kname = (f"{'fused_pair_kernel' if plan['warps_per_task'] == 2 else 'fused_step_kernel'}"
+             f"<float, V={plan['lanes']}, depth={depth}>")
     traffic = profiled_traffic().get(f"fused_step_f32_8192_depth{depth}")
     line = {
         "metric": "node-updates/s", "value": value, "unit": "node-updates/s", "n_gpus": world,
@@ -665,7 +666,8 @@ def main():
                         "ms_per_step": d_ms / ksteps, "e2e": d_nu / d_e2e,
                         "roofline": {"bound": "hbm", "achieved": d_ach, "peak": peak, "unit": "GB/s",
                                      "frac": d_ach / peak,
-                                     "kernel": f"fused_step_kernel<double, V={d_plan['lanes']}, depth={d_depth}>"},
+                                     "kernel": (f"{'fused_pair_kernel' if d_plan['warps_per_task'] == 2 else 'fused_step_kernel'}"
+                                                f"<double, V={d_plan['lanes']}, depth={d_depth}>")},
                         "clocks": d_clk}
     if rank == 0 and not args.no_cpu:
         cb = cpu_reference_sample(p)
