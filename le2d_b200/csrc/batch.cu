@@ -144,40 +144,50 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
   int* status = &ctl->status;
   unsigned u = 0;  // handoffs through the pair's queue (item indices and rows)
   int r = 0;
-  while (true) {
-    long long q;
-    const int hs = (int)(u % kHand);
-    if (producer) {
+  // The two roles run separate loops (each keeps only its own state live across its march).
+  if (producer) {
+    while (true) {
+      const int hs = (int)(u % kHand);
       unsigned long long claimed = 0;
       if (lane == 0) claimed = atomicAdd(&ctl->next, 1ULL);
-      q = (long long)__shfl_sync(0xffffffffu, claimed, 0);
+      const long long q = (long long)__shfl_sync(0xffffffffu, claimed, 0);
       const unsigned use = u / kHand;
       if (use > 0 && !march::mbar_wait(bars + kHand + hs, (use - 1) & 1, wait_ns, status)) break;
       if (lane == 0) item_q[hs] = q;
       march::mbar_arrive(bars + hs);
-    } else {
-      if (!march::mbar_wait(bars + hs, (u / kHand) & 1, wait_ns, status)) break;
-      q = item_q[hs];
-      march::mbar_arrive(bars + kHand + hs);
+      ++u;
+      if (q >= total) break;
+      while (q >= step_items[r + 1]) ++r;
+      const BatchTile bt = tiles[q - step_items[r]];
+      const BatchInst<T>& I = insts[bt.inst];
+      const int nadv = min(I.depth, I.steps - r * I.depth);  // steps this item advances
+      if (r > 0 &&
+          !wait_neighbours(done, I.tile_base, I.nstrips, I.nsegs, bt.seg, bt.strip, r, ctl, wait_ns))
+        break;
+      const int par = (I.parity + r) & 1;
+      const march::GridRef<T> g{I.buf[par], I.buf[par ^ 1], I.nx, I.ny, I.pitch, I.plane, I.far_rot};
+      const int y0 = bt.seg * I.seg_len;
+      const int y1 = min(y0 + I.seg_len, I.ny);
+      if (!march::pair_produce<T, V, kNpf, true>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
+                                                 u, nadv == 1))
+        break;
     }
-    ++u;
-    if (q >= total) break;
-    while (q >= step_items[r + 1]) ++r;
-    const BatchTile bt = tiles[q - step_items[r]];
-    const BatchInst<T>& I = insts[bt.inst];
-    const int nadv = min(I.depth, I.steps - r * I.depth);  // steps this item advances
-    if (producer && r > 0 &&
-        !wait_neighbours(done, I.tile_base, I.nstrips, I.nsegs, bt.seg, bt.strip, r, ctl, wait_ns))
-      break;
-    const int par = (I.parity + r) & 1;
-    const march::GridRef<T> g{I.buf[par], I.buf[par ^ 1], I.nx, I.ny, I.pitch, I.plane, I.far_rot};
-    const int y0 = bt.seg * I.seg_len;
-    const int y1 = min(y0 + I.seg_len, I.ny);
-    bool ok;
-    if (producer) {
-      ok = march::pair_produce<T, V, kNpf, true>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
-                                                 u, nadv == 1);
-    } else {
+  } else {
+    while (true) {
+      const int hs = (int)(u % kHand);
+      if (!march::mbar_wait(bars + hs, (u / kHand) & 1, wait_ns, status)) break;
+      const long long q = item_q[hs];
+      march::mbar_arrive(bars + kHand + hs);
+      ++u;
+      if (q >= total) break;
+      while (q >= step_items[r + 1]) ++r;
+      const BatchTile bt = tiles[q - step_items[r]];
+      const BatchInst<T>& I = insts[bt.inst];
+      const int nadv = min(I.depth, I.steps - r * I.depth);
+      const int par = (I.parity + r) & 1;
+      const march::GridRef<T> g{I.buf[par], I.buf[par ^ 1], I.nx, I.ny, I.pitch, I.plane, I.far_rot};
+      const int y0 = bt.seg * I.seg_len;
+      const int y1 = min(y0 + I.seg_len, I.ny);
       // receiver samples after the item's first and (two-step items) second step
       const long long before = I.abs_step0 + (long long)r * I.depth;
       march::RowTap<T> tap_a{nullptr, -1}, tap_b{nullptr, -1};
@@ -185,13 +195,11 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
         tap_a = march::RowTap<T>{I.trace + ((before + 1) / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
       if (I.trace != nullptr && nadv == 2 && (before + 2) % I.trace_every == 0)
         tap_b = march::RowTap<T>{I.trace + ((before + 2) / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
-      ok = march::pair_consume<T, V, kNpf, true>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
-                                                 u, nadv == 1, tap_a, tap_b);
-    }
-    if (!ok) break;
-    if (!producer) {  // the consumer wrote the tile's new state and publishes it
-      __syncwarp();
       const int tile_id = I.tile_base + bt.seg * I.nstrips + bt.strip;
+      if (!march::pair_consume<T, V, kNpf, true>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
+                                                 u, nadv == 1, tap_a, tap_b))
+        break;
+      __syncwarp();  // the consumer wrote the tile's new state and publishes it
       if (lane == 0 && !(r == 0 && tile_id == stall_plus1 - 1)) {
         __threadfence();
         st_release(done + tile_id, r + 1);
