@@ -220,6 +220,27 @@ int le2d_device_layout(const le_task *task, long long *pitch_elems, long long *p
 /* Bytes of device memory a task of this size holds (for admission control). */
 size_t le2d_task_device_bytes(int nx, int ny);
 
+/* ---- One grid over several devices (row slabs) ---------------------------------------
+ * The reference's multi-GPU step (cuda5/cuda6 le_core.cu:374-509: one process, row slabs,
+ * peer copies of the rows next to each cut).  The task's grid (its size, dt, h, material
+ * and layout; not its state) is split into `nslabs` row slabs of at least 8 rows, slab i on
+ * devices[i] (a device may hold several slabs).  Each slab keeps 4 copied rows beside every
+ * cut, steps with the same kernels as a whole task, and refreshes those rows from its
+ * neighbours after every launch, so the results are bitwise those of the whole grid.
+ * Peer access between neighbouring devices is enabled where the hardware offers it. */
+typedef struct le2d_slabs le2d_slabs;
+le2d_slabs *le2d_slabs_create(const le_task *task, int nslabs, const int *devices);
+void le2d_slabs_destroy(le2d_slabs *s);
+/* Global rows [*r0, *r1) owned by slab `slab`, and its device. */
+int le2d_slabs_rows(const le2d_slabs *s, int slab, int *r0, int *r1, int *device);
+/* The whole state from / to a host grid in the task's layout (5*nx*ny reals). */
+int le2d_slabs_upload(le2d_slabs *s, const real *src);
+int le2d_slabs_download(le2d_slabs *s, real *dst);
+/* nsteps steps (le_step semantics for ST_AOS grids, le_step_soa for ST_SOA); queued on
+ * the slabs' streams, returns at once. */
+int le2d_slabs_step_n(le2d_slabs *s, int nsteps);
+int le2d_slabs_wait(le2d_slabs *s);
+
 #ifdef __cplusplus
 }
 #endif

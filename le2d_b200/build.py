@@ -23,7 +23,8 @@ BUILD = os.path.join(PKG, "_build")
 LIBDIR = os.path.join(PKG, "lib")
 INCLUDE = os.path.join(ROOT, "include")
 
-SOURCES = ["le2d_api.cu", "step_fused.cu", "step_split.cu", "layout.cu", "diag.cu", "batch.cu", "engine.cu", "serve.cu", "diag_noalloc.cu"]
+SOURCES = ["le2d_api.cu", "step_fused.cu", "step_split.cu", "layout.cu", "diag.cu", "batch.cu", "engine.cu",
+           "serve.cu", "diag_noalloc.cu", "slabs.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

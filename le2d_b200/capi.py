@@ -47,6 +47,8 @@ EXPORTS = [
     "le2d_server_wait", "le2d_server_result", "le2d_server_times", "le2d_server_release",
     "le2d_server_stats", "le2d_now", "le2d_diagnostics_noalloc", "le2d_autotune", "le2d_autotune_reset",
     "le2d_batch_autotune", "le2d_batch_autotune_reset",
+    "le2d_slabs_create", "le2d_slabs_destroy", "le2d_slabs_rows", "le2d_slabs_upload",
+    "le2d_slabs_download", "le2d_slabs_step_n", "le2d_slabs_wait",
 ]
 
 LE2D_DIAG_NOALLOC_MAX_ROWS = 16384
@@ -181,6 +183,15 @@ class Lib:
         L.le2d_autotune_reset.argtypes = []
         L.le2d_batch_autotune.argtypes = [ctypes.c_int, ctypes.c_int, P(ctypes.c_int), P(ctypes.c_double)]
         L.le2d_batch_autotune_reset.argtypes = []
+        L.le2d_slabs_create.restype = ctypes.c_void_p
+        L.le2d_slabs_create.argtypes = [P(self.le_task), ctypes.c_int, P(ctypes.c_int)]
+        L.le2d_slabs_destroy.argtypes = [ctypes.c_void_p]
+        L.le2d_slabs_rows.argtypes = [ctypes.c_void_p, ctypes.c_int, P(ctypes.c_int), P(ctypes.c_int),
+                                      P(ctypes.c_int)]
+        L.le2d_slabs_upload.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.le2d_slabs_download.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.le2d_slabs_step_n.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.le2d_slabs_wait.argtypes = [ctypes.c_void_p]
         L.le2d_diagnostics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
                                                ctypes.c_longlong, R, R, R, R, R, ctypes.c_void_p,
                                                P(self.le2d_diag_t)]
@@ -397,6 +408,55 @@ class Batch:
 
     def set_wait_limit(self, ns: int) -> int:
         return self.lib.lib.le2d_batch_set_wait_limit(self.h, ns)
+
+
+class Slabs:
+    """le2d_slabs_*: one grid split into row slabs over several devices."""
+
+    def __init__(self, lib: Lib, task, devices):
+        self.lib = lib
+        self.n = 5 * task.n.x * task.n.y
+        devs = (ctypes.c_int * len(devices))(*devices)
+        self.h = lib.lib.le2d_slabs_create(ctypes.byref(task), len(devices), devs)
+        if not self.h:
+            raise RuntimeError("le2d_slabs_create failed")
+        self.count = len(devices)
+
+    def close(self):
+        if self.h:
+            self.lib.lib.le2d_slabs_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def rows(self, i: int):
+        r0, r1, d = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        rc = self.lib.lib.le2d_slabs_rows(self.h, i, ctypes.byref(r0), ctypes.byref(r1), ctypes.byref(d))
+        if rc:
+            raise RuntimeError(self.lib.strerror(rc))
+        return r0.value, r1.value, d.value
+
+    def upload(self, src: np.ndarray) -> int:
+        src = np.ascontiguousarray(src, dtype=self.lib.dtype)
+        assert src.size == self.n
+        return self.lib.lib.le2d_slabs_upload(self.h, src.ctypes.data)
+
+    def download(self) -> np.ndarray:
+        out = np.zeros(self.n, self.lib.dtype)
+        rc = self.lib.lib.le2d_slabs_download(self.h, out.ctypes.data)
+        if rc:
+            raise RuntimeError(self.lib.strerror(rc))
+        return out
+
+    def step_n(self, n: int) -> int:
+        return self.lib.lib.le2d_slabs_step_n(self.h, n)
+
+    def wait(self) -> int:
+        return self.lib.lib.le2d_slabs_wait(self.h)
 
 
 class Server:

@@ -124,12 +124,17 @@ struct VariantKernel {
     else
       return (size_t)kWarps * warp_elems<T, C::V, C::NPF, C::D>() * sizeof(T);
   }
-  // dynamic shared memory above 48 KB must be opted into once per kernel
+  // dynamic shared memory above 48 KB must be opted into once per kernel and device
   static void prepare() {
-    static bool done = false;
-    if (!done) {
+    static unsigned long long done = 0;  // bit d: device d (devices 0..63)
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
       cudaFuncSetAttribute(fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
-      done = true;
+      return;
+    }
+    if (!(done & (1ull << dev))) {
+      cudaFuncSetAttribute(fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+      done |= 1ull << dev;
     }
   }
   static void launch(const FusedPlan& pl, const FusedParams<T>& p, cudaStream_t s) {
@@ -191,6 +196,7 @@ struct SmemOp {
 template <typename T, int VAR>
 struct LaunchOp {
   static int run(const FusedPlan& pl, const FusedParams<T>& p, cudaStream_t s) {
+    VariantKernel<T, VAR>::prepare();  // the launching device may not have planned it
     VariantKernel<T, VAR>::launch(pl, p, s);
     return 0;
   }
