@@ -508,6 +508,46 @@ def run_serving(args):
     return 0
 
 
+def run_slabs(args):
+    """The 8192^2 solve split into row slabs (le2d_slabs_*) over the visible devices,
+    round-robin, against the same solve as one task: node-updates/s per slab count."""
+    import ctypes
+
+    rt = ctypes.CDLL("libcudart.so")
+    nd = ctypes.c_int(0)
+    ndev = max(1, nd.value) if rt.cudaGetDeviceCount(ctypes.byref(nd)) == 0 else 1
+    lib = capi.Lib("f")
+    p = workloads.single_8192() if args.time_steps is None else workloads.single_8192(args.time_steps)
+    t = new_task(lib, p)
+    rows = []
+    try:
+        ic = initial_state(lib, p, t).copy()
+        for k in [1] + [int(x) for x in args.slabs.split(",")]:
+            if k == 1:
+                assert lib.upload(t, ic) == 0
+                rc, _ = lib.step_n_timed(t, 8)
+                assert lib.upload(t, ic) == 0 and lib.wait(t) == 0
+                rc, ms = lib.step_n_timed(t, p.steps)
+                assert rc == 0
+                sec = ms * 1e-3
+                devs = [0]
+            else:
+                devs = [j % ndev for j in range(k)]
+                with capi.Slabs(lib, t, devs) as s:
+                    assert s.upload(ic) == 0
+                    assert s.step_n(8) == 0 and s.wait() == 0
+                    assert s.upload(ic) == 0
+                    t0 = time.perf_counter()
+                    assert s.step_n(p.steps) == 0 and s.wait() == 0
+                    sec = time.perf_counter() - t0
+            rows.append({"slabs": k, "devices": devs, "node_updates_s": p.node_updates / sec, "seconds": sec})
+    finally:
+        lib.le_free_task(t)
+    print(json.dumps({"metric": "slabs", "workload": f"single_8192: {p.nx}x{p.ny}, {p.steps} time steps",
+                      "visible_devices": ndev, "rows": rows}), flush=True)
+    return 0
+
+
 def run_precision(args):
     """4096x4096 precision study: FP32 vs FP64 library every 500 steps up to 4000 steps,
     FP64 energy drift, and both builds against the reference's own CPU builds after 500 steps."""
@@ -617,7 +657,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="single",
-                    choices=["single", "batched", "serving", "precision", "precision-reference"])
+                    choices=["single", "batched", "serving", "precision", "precision-reference", "slabs"])
+    ap.add_argument("--slabs", default="2,4", help="slabs: slab counts besides the whole task")
     ap.add_argument("--window", type=int, default=256, help="steps per persistent launch (batched/serving)")
     ap.add_argument("--rates", default="10,50,200,2000", help="serving: request rates per second")
     ap.add_argument("--requests", type=int, default=48, help="serving: requests per rate")
@@ -637,6 +678,8 @@ def main():
         return run_precision(args)
     if args.workload == "precision-reference":
         return run_precision_reference(args)
+    if args.workload == "slabs":
+        return run_slabs(args)
 
     world, rank, local = dist_setup()
     backend = "nccl"
