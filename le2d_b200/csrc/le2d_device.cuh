@@ -49,6 +49,33 @@ struct StepConsts {
   Sweep<T> x, y;
 };
 
+// The y-sweep constants the packed FP32 pipeline multiplies by, each duplicated into an
+// (x, y) pair, so a packed instruction can take it as one 8-byte operand from the kernel
+// parameters instead of a pair assembled in registers every row.
+struct YPairs {
+  float2 ir1, nir1, ir2, nir2;  // +-irhoc1, +-irhoc2
+  float2 k1, nk1, k2, nk2;      // +-kc1, +-kc2
+  float2 hk1, hk2, hk1rc1, hk1rc3, hk2rc2;
+};
+
+__host__ __device__ inline YPairs make_ypairs(const Sweep<float>& c) {
+  YPairs p;
+  p.ir1 = make_float2(c.irhoc1, c.irhoc1);
+  p.nir1 = make_float2(-c.irhoc1, -c.irhoc1);
+  p.ir2 = make_float2(c.irhoc2, c.irhoc2);
+  p.nir2 = make_float2(-c.irhoc2, -c.irhoc2);
+  p.k1 = make_float2(c.kc1, c.kc1);
+  p.nk1 = make_float2(-c.kc1, -c.kc1);
+  p.k2 = make_float2(c.kc2, c.kc2);
+  p.nk2 = make_float2(-c.kc2, -c.kc2);
+  p.hk1 = make_float2(c.hk1, c.hk1);
+  p.hk2 = make_float2(c.hk2, c.hk2);
+  p.hk1rc1 = make_float2(c.hk1rc1, c.hk1rc1);
+  p.hk1rc3 = make_float2(c.hk1rc3, c.hk1rc3);
+  p.hk2rc2 = make_float2(c.hk2rc2, c.hk2rc2);
+  return p;
+}
+
 template <typename T>
 __device__ __forceinline__ T tvd_eps();
 template <>

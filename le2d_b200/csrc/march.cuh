@@ -300,12 +300,11 @@ struct YPipe<float, V> {
       for (int q = 0; q < 2; ++q) p2[q][i] = nt2[q][i] = na2[q][i] = q2[q][i] = d2[q][i] = c2[q][i] = f2(0.f, 0.f);
   }
 
+  // The constants come as pairs (YPairs); the Sweep overloads pair them up in registers.
   __device__ __forceinline__ void left(const float (&f)[NF][V], const float (&pvy)[V],
                                        const float (&psyy)[V], const float (&pvx)[V],
-                                       const float (&psxy)[V], const Sweep<float>& cy) {
+                                       const float (&psxy)[V], const YPairs& yc) {
     const float2 m1 = f2(-1.f, -1.f), eps = f2(1e-6f, 1e-6f);
-    const float2 nir1 = f2(-cy.irhoc1, -cy.irhoc1), ir1 = f2(cy.irhoc1, cy.irhoc1);
-    const float2 nir2 = f2(-cy.irhoc2, -cy.irhoc2), ir2 = f2(cy.irhoc2, cy.irhoc2);
 #pragma unroll
     for (int i = 0; i < P; ++i) {
       const int a = 2 * i, b = 2 * i + 1;
@@ -313,16 +312,15 @@ struct YPipe<float, V> {
       const float2 dsn = fma2(f2(psyy[a], psyy[b]), m1, f2(f[SYY][a], f[SYY][b]));
       const float2 dvt = fma2(f2(pvx[a], pvx[b]), m1, f2(f[VX][a], f[VX][b]));
       const float2 dsx = fma2(f2(psxy[a], psxy[b]), m1, f2(f[SXY][a], f[SXY][b]));
-      const float2 d[4] = {fma2(dsn, nir1, dvn), fma2(dsn, ir1, dvn), fma2(dsx, nir2, dvt),
-                           fma2(dsx, ir2, dvt)};
+      const float2 d[4] = {fma2(dsn, yc.nir1, dvn), fma2(dsn, yc.ir1, dvn), fma2(dsx, yc.nir2, dvt),
+                           fma2(dsx, yc.ir2, dvt)};
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const float k = q ? cy.kc2 : cy.kc1;
         dfw[q][i] = d[2 * q];
         const float2 dd = d[2 * q + 1];
         const float2 q1 = fma2(dd, m1, eps);  // eps - D
         const float2 phi = superbee2(ratio2(q1, q2[q][i]));
-        const float2 ps = mul2(f2(k, k), phi), nps = mul2(f2(-k, -k), phi);
+        const float2 ps = mul2(q ? yc.k2 : yc.k1, phi), nps = mul2(q ? yc.nk2 : yc.nk1, phi);
         bo[q][i] = fma2(nps, d2[q][i], c2[q][i]);  // c - psi' D_{m-2}
         c2[q][i] = fma2(ps, d2[q][i], dd);         // D + psi' D_{m-2}
         d2[q][i] = dd;
@@ -330,8 +328,13 @@ struct YPipe<float, V> {
       }
     }
   }
+  __device__ __forceinline__ void left(const float (&f)[NF][V], const float (&pvy)[V],
+                                       const float (&psyy)[V], const float (&pvx)[V],
+                                       const float (&psxy)[V], const Sweep<float>& cy) {
+    left(f, pvy, psyy, pvx, psxy, make_ypairs(cy));
+  }
 
-  __device__ __forceinline__ void apply(float (&gf)[NF][V], const Sweep<float>& cy) const {
+  __device__ __forceinline__ void apply(float (&gf)[NF][V], const YPairs& yc) const {
     const float2 m1 = f2(-1.f, -1.f);
 #pragma unroll
     for (int i = 0; i < P; ++i) {
@@ -340,11 +343,11 @@ struct YPipe<float, V> {
       const float2 p1 = add2(bo[0][i], na2[0][i]);     // B2 - A1
       const float2 s3 = fma2(na2[1][i], m1, bo[1][i]);  // A3 + B4
       const float2 p3 = add2(bo[1][i], na2[1][i]);     // B4 - A3
-      const float2 vy = fma2(f2(cy.hk1, cy.hk1), s1, f2(gf[VY][a], gf[VY][b]));
-      const float2 vx = fma2(f2(cy.hk2, cy.hk2), s3, f2(gf[VX][a], gf[VX][b]));
-      const float2 syy = fma2(f2(cy.hk1rc1, cy.hk1rc1), p1, f2(gf[SYY][a], gf[SYY][b]));
-      const float2 sxx = fma2(f2(cy.hk1rc3, cy.hk1rc3), p1, f2(gf[SXX][a], gf[SXX][b]));
-      const float2 sxy = fma2(f2(cy.hk2rc2, cy.hk2rc2), p3, f2(gf[SXY][a], gf[SXY][b]));
+      const float2 vy = fma2(yc.hk1, s1, f2(gf[VY][a], gf[VY][b]));
+      const float2 vx = fma2(yc.hk2, s3, f2(gf[VX][a], gf[VX][b]));
+      const float2 syy = fma2(yc.hk1rc1, p1, f2(gf[SYY][a], gf[SYY][b]));
+      const float2 sxx = fma2(yc.hk1rc3, p1, f2(gf[SXX][a], gf[SXX][b]));
+      const float2 sxy = fma2(yc.hk2rc2, p3, f2(gf[SXY][a], gf[SXY][b]));
       gf[VY][a] = vy.x; gf[VY][b] = vy.y;
       gf[VX][a] = vx.x; gf[VX][b] = vx.y;
       gf[SYY][a] = syy.x; gf[SYY][b] = syy.y;
@@ -352,24 +355,27 @@ struct YPipe<float, V> {
       gf[SXY][a] = sxy.x; gf[SXY][b] = sxy.y;
     }
   }
+  __device__ __forceinline__ void apply(float (&gf)[NF][V], const Sweep<float>& cy) const {
+    apply(gf, make_ypairs(cy));
+  }
 
-  __device__ __forceinline__ void right(const Sweep<float>& cy) {
+  __device__ __forceinline__ void right(const YPairs& yc) {
     const float2 eps = f2(1e-6f, 1e-6f);
 #pragma unroll
     for (int i = 0; i < P; ++i) {
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const float k = q ? cy.kc2 : cy.kc1;
         const float2 dd = dfw[q][i];
         const float2 p1 = add2(dd, eps);
         const float2 phi = superbee2(ratio2(p2[q][i], p1));
-        const float2 ps = mul2(f2(k, k), phi), nps = mul2(f2(-k, -k), phi);
+        const float2 ps = mul2(q ? yc.k2 : yc.k1, phi), nps = mul2(q ? yc.nk2 : yc.nk1, phi);
         na2[q][i] = fma2(ps, dd, nt2[q][i]);  // -(t_{m-2} - psi D)
         nt2[q][i] = fma2(nps, dd, dd);        // -(psi - 1) D
         p2[q][i] = p1;
       }
     }
   }
+  __device__ __forceinline__ void right(const Sweep<float>& cy) { right(make_ypairs(cy)); }
 };
 
 // Advances one tile -- strip `strip` (32*V columns, halo lanes included), rows [y0, y1) --

@@ -57,10 +57,11 @@ __device__ __forceinline__ void clamp_columns(T (&v)[NF][V], int xs, int col0, i
 }
 
 // One x-swept row into a y-pipeline: store it in the ring slot, read it and the previous
-// row back (aligned loads), advance the left-moving part.
-template <typename T, int V>
+// row back (aligned loads), advance the left-moving part.  `cy`: the y-sweep constants
+// (Sweep, or YPairs for the FP32 pipeline).
+template <typename T, int V, typename CY>
 __device__ __forceinline__ void ring_left(YPipe<T, V>& yp, T (&f)[NF][V], T* ring, int slot,
-                                          const Sweep<T>& cy) {
+                                          const CY& cy) {
   using VT = typename Vec<T, V>::type;
   constexpr int kIn = 32 * V;
   constexpr int kRow = NF * kIn;
@@ -81,9 +82,9 @@ __device__ __forceinline__ void ring_left(YPipe<T, V>& yp, T (&f)[NF][V], T* rin
 }
 
 // The row two above, completed: fields from the ring plus the pipeline's increments.
-template <typename T, int V>
+template <typename T, int V, typename CY>
 __device__ __forceinline__ void ring_output(const YPipe<T, V>& yp, T (&out)[NF][V], const T* ring,
-                                            int slot, const Sweep<T>& cy) {
+                                            int slot, const CY& cy) {
   using VT = typename Vec<T, V>::type;
   constexpr int kIn = 32 * V;
   constexpr int kRow = NF * kIn;

@@ -8,6 +8,8 @@
 // block is just kWarps of them sharing the launch.  Variants of temporal-block depth 2
 // advance each tile by two steps per launch, on one warp (march2.cuh) or on a producer /
 // consumer warp pair (march_pair.cuh).
+#include <type_traits>
+
 #include "march_pair.cuh"
 
 namespace le2d {
@@ -19,8 +21,13 @@ struct FusedParams {
   march::GridRef<T> g;
   int nstrips, seg_len, ntasks;
   StepConsts<T> c;
+  YPairs yq;     // FP32: c.y as pairs for the packed y-pipeline
   PairCtl pair;  // warp-pair waits
 };
+
+// The y-sweep constants the interior loops hand to the y-pipeline: pairs for FP32.
+__device__ __forceinline__ const YPairs& ycons(const FusedParams<float>& p) { return p.yq; }
+__device__ __forceinline__ const Sweep<double>& ycons(const FusedParams<double>& p) { return p.c.y; }
 
 constexpr int kWarps = 4;  // warps per block
 
@@ -47,15 +54,15 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) fused_step_kernel(const Fus
                                                 march::RowTap<T>{nullptr, -1});
 }
 
-// Two-step tiles on warp pairs: kWarps / 2 pairs per block, each with its own shared
+// Two-step tiles on warp pairs: W / 2 pairs per block, each with its own shared
 // memory and queue barriers.  The barriers are initialised before the block's barrier, so
 // both warps of a pair see them, and the pair leaves together (same tile).
-template <typename T, int V, int MINB, int NPF>
-__global__ void __launch_bounds__(kWarps * 32, MINB) fused_pair_kernel(const FusedParams<T> p) {
+template <typename T, int V, int MINB, int NPF, int W, int F>
+__global__ void __launch_bounds__(W * 32, MINB) fused_pair_kernel(const FusedParams<T> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int kPairs = kWarps / 2;
+  constexpr int kPairs = W / 2;
   const int wib = threadIdx.x >> 5;
-  const int pair = wib >> 1;
+  const int pair = kPairs == 1 ? 0 : wib >> 1;
   unsigned char* base = smem_raw + pair * march::pair_smem_bytes<T, V, NPF>();
   unsigned long long* bars =
       reinterpret_cast<unsigned long long*>(base + march::pair_smem_elems<T, V, NPF>() * sizeof(T));
@@ -71,6 +78,18 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) fused_pair_kernel(const Fus
   T* smem = reinterpret_cast<T*>(base);
   unsigned u = 0;
   const march::RowTap<T> no_tap{nullptr, -1};
+  if constexpr (F == 1 && NPF == 2) {  // interior tiles on the lean loops
+    const int xs = strip * strip_cols2(V) - halo_lanes2(V) * V;
+    if (march::tile_is_interior<T, V>(p.g, xs, y0, y1)) {
+      if ((wib & 1) == 0)
+        march::pair_produce_interior<T, V>(p.g, p.c.x, ycons(p), xs, y0, y1, smem, bars,
+                                           p.pair.wait_ns, p.pair.status, u);
+      else
+        march::pair_consume_interior<T, V>(p.g, p.c.x, ycons(p), xs, y0, y1, smem, bars,
+                                           p.pair.wait_ns, p.pair.status, u);
+      return;
+    }
+  }
   if ((wib & 1) == 0)
     march::pair_produce<T, V, NPF, false>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns,
                                           p.pair.status, u, false);
@@ -85,42 +104,47 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) fused_pair_kernel(const Fus
 // the temporal-block depth D (steps per launch) and P = 1 for two-step tiles on warp pairs.
 template <typename T, int VAR>
 struct VariantCfg;
-template <> struct VariantCfg<float, 0> { static constexpr int V = 4, MINB = 3, NPF = 2, D = 1, P = 0; };
-template <> struct VariantCfg<float, 1> { static constexpr int V = 4, MINB = 3, NPF = 3, D = 1, P = 0; };
-template <> struct VariantCfg<float, 2> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 1, P = 0; };
-template <> struct VariantCfg<float, 3> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 1, P = 0; };
-template <> struct VariantCfg<float, 4> { static constexpr int V = 2, MINB = 4, NPF = 3, D = 1, P = 0; };
-template <> struct VariantCfg<float, 5> { static constexpr int V = 4, MINB = 2, NPF = 2, D = 2, P = 0; };
-template <> struct VariantCfg<float, 6> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 2, P = 0; };
-template <> struct VariantCfg<float, 7> { static constexpr int V = 2, MINB = 3, NPF = 3, D = 2, P = 0; };
-template <> struct VariantCfg<float, 8> { static constexpr int V = 2, MINB = 5, NPF = 2, D = 2, P = 0; };
-template <> struct VariantCfg<float, 9> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 2, P = 1; };
-template <> struct VariantCfg<float, 10> { static constexpr int V = 4, MINB = 3, NPF = 3, D = 2, P = 1; };
-template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 1, P = 0; };
-template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 1, P = 0; };
-template <> struct VariantCfg<double, 2> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 1, P = 0; };
-template <> struct VariantCfg<double, 3> { static constexpr int V = 1, MINB = 4, NPF = 3, D = 1, P = 0; };
-template <> struct VariantCfg<double, 4> { static constexpr int V = 1, MINB = 5, NPF = 2, D = 1, P = 0; };
-template <> struct VariantCfg<double, 5> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 2, P = 0; };
-template <> struct VariantCfg<double, 6> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 2, P = 0; };
-template <> struct VariantCfg<double, 7> { static constexpr int V = 1, MINB = 3, NPF = 3, D = 2, P = 0; };
-template <> struct VariantCfg<double, 8> { static constexpr int V = 1, MINB = 5, NPF = 2, D = 2, P = 0; };
-template <> struct VariantCfg<double, 9> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 2, P = 1; };
-template <> struct VariantCfg<double, 10> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 2, P = 1; };
-constexpr int kVariants = 11;
+template <> struct VariantCfg<float, 0> { static constexpr int V = 4, MINB = 3, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<float, 1> { static constexpr int V = 4, MINB = 3, NPF = 3, D = 1, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<float, 2> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<float, 3> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<float, 4> { static constexpr int V = 2, MINB = 4, NPF = 3, D = 1, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<float, 5> { static constexpr int V = 4, MINB = 2, NPF = 2, D = 2, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<float, 6> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 2, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<float, 7> { static constexpr int V = 2, MINB = 3, NPF = 3, D = 2, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<float, 8> { static constexpr int V = 2, MINB = 5, NPF = 2, D = 2, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<float, 9> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 2, P = 1, W = 4, F = 0; };
+template <> struct VariantCfg<float, 10> { static constexpr int V = 4, MINB = 3, NPF = 3, D = 2, P = 1, W = 4, F = 0; };
+template <> struct VariantCfg<float, 11> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 2, P = 1, W = 4, F = 1; };
+template <> struct VariantCfg<float, 12> { static constexpr int V = 4, MINB = 8, NPF = 2, D = 2, P = 1, W = 2, F = 1; };
+template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<double, 2> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<double, 3> { static constexpr int V = 1, MINB = 4, NPF = 3, D = 1, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<double, 4> { static constexpr int V = 1, MINB = 5, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<double, 5> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 2, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<double, 6> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 2, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<double, 7> { static constexpr int V = 1, MINB = 3, NPF = 3, D = 2, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<double, 8> { static constexpr int V = 1, MINB = 5, NPF = 2, D = 2, P = 0, W = 4, F = 0; };
+template <> struct VariantCfg<double, 9> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 2, P = 1, W = 4, F = 0; };
+template <> struct VariantCfg<double, 10> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 2, P = 1, W = 4, F = 0; };
+template <> struct VariantCfg<double, 11> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 2, P = 1, W = 4, F = 1; };
+template <> struct VariantCfg<double, 12> { static constexpr int V = 2, MINB = 6, NPF = 2, D = 2, P = 1, W = 2, F = 1; };
+constexpr int kVariants = 13;
 
 template <typename T, int VAR>
 struct VariantKernel {
   using C = VariantCfg<T, VAR>;
+  static_assert(C::P == 1 || (C::F == 0 && C::W == kWarps), "lean loops and block size: warp pairs only");
   static void* fn() {
     if constexpr (C::P == 1)
-      return (void*)fused_pair_kernel<T, C::V, C::MINB, C::NPF>;
+      return (void*)fused_pair_kernel<T, C::V, C::MINB, C::NPF, C::W, C::F>;
     else
       return (void*)fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D>;
   }
   static size_t smem() {
     if constexpr (C::P == 1)
-      return (size_t)(kWarps / 2) * march::pair_smem_bytes<T, C::V, C::NPF>();
+      return (size_t)(C::W / 2) * march::pair_smem_bytes<T, C::V, C::NPF>();
     else
       return (size_t)kWarps * warp_elems<T, C::V, C::NPF, C::D>() * sizeof(T);
   }
@@ -139,7 +163,7 @@ struct VariantKernel {
   }
   static void launch(const FusedPlan& pl, const FusedParams<T>& p, cudaStream_t s) {
     if constexpr (C::P == 1)
-      fused_pair_kernel<T, C::V, C::MINB, C::NPF><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
+      fused_pair_kernel<T, C::V, C::MINB, C::NPF, C::W, C::F><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
     else
       fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
   }
@@ -158,6 +182,8 @@ R with_variant(int var, A&&... a) {
     case 8: return Op<T, 8>::run(a...);
     case 9: return Op<T, 9>::run(a...);
     case 10: return Op<T, 10>::run(a...);
+    case 11: return Op<T, 11>::run(a...);
+    case 12: return Op<T, 12>::run(a...);
     default: return Op<T, 0>::run(a...);
   }
 }
@@ -175,15 +201,20 @@ struct PairOp {
   static int run() { return VariantCfg<T, VAR>::P; }
 };
 template <typename T, int VAR>
+struct WarpsOp {
+  static int run() { return VariantCfg<T, VAR>::W; }
+};
+template <typename T, int VAR>
 struct ResidentOp {
   static int run(int device) {
     int sms = 0, per_sm = 0;
     VariantKernel<T, VAR>::prepare();
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, VariantKernel<T, VAR>::fn(), kWarps * 32,
+    constexpr int W = VariantCfg<T, VAR>::W;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, VariantKernel<T, VAR>::fn(), W * 32,
                                                       VariantKernel<T, VAR>::smem()) != cudaSuccess)
       return 0;
-    return sms * per_sm * kWarps;
+    return sms * per_sm * W;
   }
 };
 template <typename T, int VAR>
@@ -245,8 +276,9 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
   pl.seg_len = seg;
   pl.nsegs = (ny + seg - 1) / seg;
   pl.ntasks = pl.nstrips * pl.nsegs;
-  pl.threads = kWarps * 32;
-  const int tasks_per_block = kWarps / pl.warps_per_task;
+  const int warps = with_variant<T, WarpsOp, int>(pl.variant);
+  pl.threads = warps * 32;
+  const int tasks_per_block = warps / pl.warps_per_task;
   pl.blocks = (pl.ntasks + tasks_per_block - 1) / tasks_per_block;
   pl.smem = with_variant<T, SmemOp, size_t>(pl.variant);
   return pl;
@@ -265,6 +297,8 @@ cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pi
   p.seg_len = plan.seg_len;
   p.ntasks = plan.ntasks;
   p.c = c;
+  p.yq = YPairs{};
+  if constexpr (std::is_same<T, float>::value) p.yq = make_ypairs(c.y);
   with_variant<T, LaunchOp, int>(plan.variant, plan, p, s);
   return cudaGetLastError();
 }

@@ -243,6 +243,37 @@ def test_temporal_blocking_edges(libs, prec):
 
 
 @pytest.mark.parametrize("prec", ["f", "d"])
+def test_interior_tiles_lean_loops(libs, prec):
+    """Grids wide and tall enough that most two-step tiles are interior (strip inside the
+    grid, 4 rows of margin above and below), which the lean interior loops take, with even
+    and odd segment lengths: bitwise equal to one step per launch."""
+    lib = libs[prec]
+    vs = variants(lib)
+    two = [v for v, d in vs.items() if d == 2]
+    one = [v for v, d in vs.items() if d == 1][0]
+    rng = np.random.default_rng(23)
+    for nx, ny, steps in ((517, 301, 10), (1000, 97, 7)):
+        c = dict(nx=nx, ny=ny, hx=1.0, hy=0.9, c1=2.0, c2=1.1, rho=1.3, dt=0.2, stype=ST_AOS)
+        g0 = rng.uniform(-1, 1, size=5 * nx * ny).astype(lib.dtype)
+        ref = None
+        for var, seg in [(one, 0)] + [(v, s) for v in two for s in (0, 8, 9, 40)]:
+            t = make_task(lib, c)
+            try:
+                assert lib.set_variant(t, var, seg) == 0
+                assert lib.upload(t, g0.copy()) == 0
+                assert lib.step_n(t, steps) == 0
+                got = np.zeros_like(g0)
+                assert lib.download(t, got) == 0
+                assert lib.last_error(t) == 0
+            finally:
+                lib.le_free_task(t)
+            if ref is None:
+                ref = got
+            else:
+                assert got.tobytes() == ref.tobytes(), (nx, ny, var, seg)
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
 def test_uniform_state_is_fixed_point(libs, prec):
     c = dict(nx=257, ny=131, hx=1.0, hy=1.0, c1=2.0, c2=1.0, rho=1.0, dt=0.25, stype=ST_AOS)
     g0 = np.tile(np.array([0.3, -0.2, 1.5, 0.25, -0.7], libs[prec].dtype), 257 * 131)
