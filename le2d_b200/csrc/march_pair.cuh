@@ -98,10 +98,14 @@ template <typename T, int V, int NPF>
 __host__ __device__ constexpr int pair_smem_elems() {
   return (NPF + 3 + kHand + 3) * NF * 32 * V;
 }
+// Rounded up to 16 bytes: the next pair of the block starts where this one ends, and its
+// rows are read and written with 16-byte vector accesses.
 template <typename T, int V, int NPF>
 __host__ __device__ constexpr int pair_smem_bytes() {
-  return pair_smem_elems<T, V, NPF>() * (int)sizeof(T) + 2 * kHand * 8 + kHand * 8;
+  return (pair_smem_elems<T, V, NPF>() * (int)sizeof(T) + 2 * kHand * 8 + kHand * 8 + 15) / 16 * 16;
 }
+static_assert(pair_smem_bytes<float, 4, 2>() % 16 == 0 && pair_smem_bytes<double, 2, 3>() % 16 == 0,
+              "pair shared memory must keep 16-byte alignment");
 
 // How many rows of step B's stencil step-A row ka stands for (tile rows [y0, y1)):
 // step B reads rows [y0-2, y1+2) clamped to [0, ny).  A one-step tile hands over its own
@@ -161,7 +165,7 @@ __device__ __forceinline__ void store_if(bool p, double* a, const double& v) {
 // recomputing them and store with predicates: about 8 % fewer instructions per node-update
 // with a loop no larger than the general one (a loop over two rows, which would let the
 // y-pipeline's replaced states alternate instead of being copied, measured slower: it no
-// longer fits the instruction cache).  Two-slot input ring only (NPF = 2).
+// longer fits the instruction cache).
 template <typename T, int V>
 __device__ __forceinline__ bool tile_is_interior(const GridRef<T>& g, int xs, int y0, int y1) {
   return xs >= 0 && xs + 32 * V <= g.nx && y0 >= 4 && y1 + 4 <= g.ny;
@@ -176,14 +180,14 @@ __device__ __forceinline__ void fetch_interior(T* slot, const T* row, long long 
 }
 
 // `cy`: the y-sweep constants (Sweep, or YPairs for the FP32 pipeline).
-template <typename T, int V, typename CY>
+template <typename T, int V, int NPF, typename CY>
 __device__ __forceinline__ bool pair_produce_interior(const GridRef<T>& g, const Sweep<T>& cx,
                                                       const CY& cy, int xs, int y0, int y1,
                                                       T* smem_pair, unsigned long long* bars,
                                                       unsigned long long wait_ns, int* status,
                                                       unsigned& u) {
   using VT = typename Vec<T, V>::type;
-  constexpr int NPF = 2;
+  static_assert(NPF >= 2, "the input ring needs at least the current and the next row");
   constexpr int kIn = 32 * V;
   constexpr int kRow = NF * kIn;
   const int lane = threadIdx.x & 31;
@@ -199,19 +203,22 @@ __device__ __forceinline__ bool pair_produce_interior(const GridRef<T>& g, const
 #pragma unroll
   for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(a_ring + 2 * kRow + k * kIn) = VT{};
   const T* next = g.src + (long long)(y0 - 4) * g.pitch + xs + lane * V;  // next row to fetch
-  fetch_interior<T, V>(in_ring, next, g.plane);
-  next += g.pitch;
+#pragma unroll
+  for (int j = 0; j < NPF - 1; ++j) {
+    fetch_interior<T, V>(in_ring + j * kRow, next, g.plane);
+    next += g.pitch;
+  }
   int aslot = 0;
-  int islot = 0;  // input slot of row m
+  int islot = 0;  // input slot of row m; row m+NPF-1 goes to the slot before it
   bool ok = true;
   for (int m = y0 - 4; m < mend; ++m) {
-    if (m + 1 < mend) {
-      fetch_interior<T, V>(in_ring + (islot ^ 1) * kRow, next, g.plane);
+    if (m + NPF - 1 < mend) {
+      fetch_interior<T, V>(in_ring + (islot == 0 ? NPF - 1 : islot - 1) * kRow, next, g.plane);
       next += g.pitch;
     } else {
-      cp_async_commit();
+      cp_async_commit();  // keep one group per row
     }
-    cp_async_wait<1>();
+    cp_async_wait<NPF - 1>();
     T f[NF][V];
 #pragma unroll
     for (int k = 0; k < NF; ++k) unpack(*reinterpret_cast<const VT*>(in_ring + islot * kRow + k * kIn), f[k]);
@@ -233,21 +240,20 @@ __device__ __forceinline__ bool pair_produce_interior(const GridRef<T>& g, const
       ++u;
     }
     ya.right(cy);
-    islot ^= 1;
+    islot = islot + 1 == NPF ? 0 : islot + 1;
     aslot = aslot == 2 ? 0 : aslot + 1;
   }
   cp_async_wait<0>();  // nothing of this warp's in flight when it leaves (also after a break)
   return ok;
 }
 
-template <typename T, int V, typename CY>
+template <typename T, int V, int NPF, typename CY>
 __device__ __forceinline__ bool pair_consume_interior(const GridRef<T>& g, const Sweep<T>& cx,
                                                       const CY& cy, int xs, int y0, int y1,
                                                       T* smem_pair, unsigned long long* bars,
                                                       unsigned long long wait_ns, int* status,
                                                       unsigned& u) {
   using VT = typename Vec<T, V>::type;
-  constexpr int NPF = 2;
   constexpr int H2 = halo_lanes2(V);
   constexpr int kIn = 32 * V;
   constexpr int kRow = NF * kIn;

@@ -66,11 +66,12 @@ __global__ void __launch_bounds__(W * 32, MINB) fused_pair_kernel(const FusedPar
   unsigned char* base = smem_raw + pair * march::pair_smem_bytes<T, V, NPF>();
   unsigned long long* bars =
       reinterpret_cast<unsigned long long*>(base + march::pair_smem_elems<T, V, NPF>() * sizeof(T));
-  if ((wib & 1) == 0) march::pair_init<T, V>(bars);
+  const bool producer = (wib & 1) == 0;
+  if (producer) march::pair_init<T, V>(bars);
   __syncthreads();
   const int task = blockIdx.x * kPairs + pair;
   if (task >= p.ntasks) return;  // both warps of the pair
-  if (task == p.pair.stall_task && (wib & 1) == 0) return;  // test hook
+  if (task == p.pair.stall_task && producer) return;  // test hook
   const int strip = task % p.nstrips;
   const int seg = task / p.nstrips;
   const int y0 = seg * p.seg_len;
@@ -78,19 +79,19 @@ __global__ void __launch_bounds__(W * 32, MINB) fused_pair_kernel(const FusedPar
   T* smem = reinterpret_cast<T*>(base);
   unsigned u = 0;
   const march::RowTap<T> no_tap{nullptr, -1};
-  if constexpr (F == 1 && NPF == 2) {  // interior tiles on the lean loops
+  if constexpr (F == 1) {  // interior tiles on the lean loops
     const int xs = strip * strip_cols2(V) - halo_lanes2(V) * V;
     if (march::tile_is_interior<T, V>(p.g, xs, y0, y1)) {
-      if ((wib & 1) == 0)
-        march::pair_produce_interior<T, V>(p.g, p.c.x, ycons(p), xs, y0, y1, smem, bars,
-                                           p.pair.wait_ns, p.pair.status, u);
+      if (producer)
+        march::pair_produce_interior<T, V, NPF>(p.g, p.c.x, ycons(p), xs, y0, y1, smem, bars,
+                                                p.pair.wait_ns, p.pair.status, u);
       else
-        march::pair_consume_interior<T, V>(p.g, p.c.x, ycons(p), xs, y0, y1, smem, bars,
-                                           p.pair.wait_ns, p.pair.status, u);
+        march::pair_consume_interior<T, V, NPF>(p.g, p.c.x, ycons(p), xs, y0, y1, smem, bars,
+                                                p.pair.wait_ns, p.pair.status, u);
       return;
     }
   }
-  if ((wib & 1) == 0)
+  if (producer)
     march::pair_produce<T, V, NPF, false>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns,
                                           p.pair.status, u, false);
   else
