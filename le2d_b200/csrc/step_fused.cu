@@ -23,7 +23,40 @@ struct FusedParams {
   StepConsts<T> c;
   YPairs yq;     // FP32: c.y as pairs for the packed y-pipeline
   PairCtl pair;  // warp-pair waits
+  // interior tiles: strips [s_lo, s_hi) x segments [g_lo, g_hi) (empty when lo >= hi)
+  int s_lo, s_hi, g_lo, g_hi;
 };
+
+// Tile of a task when the interior tiles come first (in segment-major order) and the
+// boundary tiles -- the segments above g_lo and from g_hi on, and the strips outside
+// [s_lo, s_hi) of the segments between -- after them.
+template <typename T>
+__device__ __forceinline__ void interior_first(const FusedParams<T>& p, int task, int& strip, int& seg) {
+  const int ni = p.s_hi - p.s_lo, ng = p.g_hi - p.g_lo;
+  if (task < ni * ng) {
+    seg = p.g_lo + task / ni;
+    strip = p.s_lo + task % ni;
+    return;
+  }
+  int k = task - ni * ng;
+  const int top = p.g_lo * p.nstrips;
+  if (k < top) {
+    seg = k / p.nstrips;
+    strip = k % p.nstrips;
+    return;
+  }
+  k -= top;
+  const int side = p.nstrips - ni;  // boundary strips of a middle segment
+  if (k < ng * side) {
+    seg = p.g_lo + k / side;
+    const int j = k % side;
+    strip = j < p.s_lo ? j : p.s_hi + (j - p.s_lo);
+    return;
+  }
+  k -= ng * side;
+  seg = p.g_hi + k / p.nstrips;
+  strip = k % p.nstrips;
+}
 
 // The y-sweep constants the interior loops hand to the y-pipeline: pairs for FP32.
 __device__ __forceinline__ const YPairs& ycons(const FusedParams<float>& p) { return p.yq; }
@@ -72,14 +105,15 @@ __global__ void __launch_bounds__(W * 32, MINB) fused_pair_kernel(const FusedPar
   const int task = blockIdx.x * kPairs + pair;
   if (task >= p.ntasks) return;  // both warps of the pair
   if (task == p.pair.stall_task && producer) return;  // test hook
-  const int strip = task % p.nstrips;
-  const int seg = task / p.nstrips;
+  int strip = task % p.nstrips;
+  int seg = task / p.nstrips;
+  if constexpr (F == 2) interior_first(p, task, strip, seg);
   const int y0 = seg * p.seg_len;
   const int y1 = min(y0 + p.seg_len, p.g.ny);
   T* smem = reinterpret_cast<T*>(base);
   unsigned u = 0;
   const march::RowTap<T> no_tap{nullptr, -1};
-  if constexpr (F == 1) {  // interior tiles on the lean loops
+  if constexpr (F >= 1) {  // interior tiles on the lean loops
     const int xs = strip * strip_cols2(V) - halo_lanes2(V) * V;
     if (march::tile_is_interior<T, V>(p.g, xs, y0, y1)) {
       if (producer)
@@ -102,7 +136,10 @@ __global__ void __launch_bounds__(W * 32, MINB) fused_pair_kernel(const FusedPar
 // Compiled variants: columns per lane V (one 16- or 8-byte access per field), the
 // minimum resident blocks per SM handed to the register allocator, the depth of the
 // shared-memory input ring (NPF - 1 rows are in flight ahead of the row being swept),
-// the temporal-block depth D (steps per launch) and P = 1 for two-step tiles on warp pairs.
+// the temporal-block depth D (steps per launch), P = 1 for two-step tiles on warp pairs,
+// warps per block W, and F: 1 = interior tiles on the lean loops, 2 = the same with the
+// interior tiles dealt out first (so the general loops, which boundary tiles take, run
+// beside the lean ones on an SM only at the end of the launch).
 template <typename T, int VAR>
 struct VariantCfg;
 template <> struct VariantCfg<float, 0> { static constexpr int V = 4, MINB = 3, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
@@ -118,6 +155,7 @@ template <> struct VariantCfg<float, 9> { static constexpr int V = 4, MINB = 4, 
 template <> struct VariantCfg<float, 10> { static constexpr int V = 4, MINB = 3, NPF = 3, D = 2, P = 1, W = 4, F = 0; };
 template <> struct VariantCfg<float, 11> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 2, P = 1, W = 4, F = 1; };
 template <> struct VariantCfg<float, 12> { static constexpr int V = 4, MINB = 8, NPF = 2, D = 2, P = 1, W = 2, F = 1; };
+template <> struct VariantCfg<float, 13> { static constexpr int V = 4, MINB = 8, NPF = 2, D = 2, P = 1, W = 2, F = 2; };
 template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
 template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
 template <> struct VariantCfg<double, 2> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
@@ -131,7 +169,8 @@ template <> struct VariantCfg<double, 9> { static constexpr int V = 2, MINB = 3,
 template <> struct VariantCfg<double, 10> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 2, P = 1, W = 4, F = 0; };
 template <> struct VariantCfg<double, 11> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 2, P = 1, W = 4, F = 1; };
 template <> struct VariantCfg<double, 12> { static constexpr int V = 2, MINB = 6, NPF = 2, D = 2, P = 1, W = 2, F = 1; };
-constexpr int kVariants = 13;
+template <> struct VariantCfg<double, 13> { static constexpr int V = 2, MINB = 6, NPF = 2, D = 2, P = 1, W = 2, F = 2; };
+constexpr int kVariants = 14;
 
 template <typename T, int VAR>
 struct VariantKernel {
@@ -185,6 +224,7 @@ R with_variant(int var, A&&... a) {
     case 10: return Op<T, 10>::run(a...);
     case 11: return Op<T, 11>::run(a...);
     case 12: return Op<T, 12>::run(a...);
+    case 13: return Op<T, 13>::run(a...);
     default: return Op<T, 0>::run(a...);
   }
 }
@@ -300,6 +340,16 @@ cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pi
   p.c = c;
   p.yq = YPairs{};
   if constexpr (std::is_same<T, float>::value) p.yq = make_ypairs(c.y);
+  {  // the interior tiles' rectangle (tile_is_interior for two-step strips and segments)
+    const int V = plan.lanes, H = halo_lanes2(V) * V, out = strip_cols2(V), L = plan.seg_len;
+    p.s_lo = (H + out - 1) / out;
+    p.s_hi = nx - 32 * V + H >= 0 ? (nx - 32 * V + H) / out + 1 : 0;
+    if (p.s_hi > plan.nstrips) p.s_hi = plan.nstrips;
+    p.g_lo = (4 + L - 1) / L;
+    p.g_hi = ny >= 4 ? (ny - 4) / L : 0;
+    if (p.s_hi < p.s_lo) p.s_hi = p.s_lo;
+    if (p.g_hi < p.g_lo) p.g_hi = p.g_lo;
+  }
   with_variant<T, LaunchOp, int>(plan.variant, plan, p, s);
   return cudaGetLastError();
 }
