@@ -294,6 +294,66 @@ __device__ __forceinline__ bool pair_consume_interior(const GridRef<T>& g, const
   return true;
 }
 
+// One step on one warp (march_tile) for an interior tile of a one-step launch: the strip
+// inside [0, nx) and the rows [y0-2, y1+2) it reads inside [0, ny), so no clamps, row
+// addresses stepped, predicated stores.
+template <typename T, int V>
+__device__ __forceinline__ bool tile_is_interior1(const GridRef<T>& g, int xs, int y0, int y1) {
+  return xs >= 0 && xs + 32 * V <= g.nx && y0 >= 2 && y1 + 2 <= g.ny;
+}
+
+template <typename T, int V, int NPF>
+__device__ __forceinline__ void march_tile_interior(const GridRef<T>& g, const StepConsts<T>& c, int xs,
+                                                    int y0, int y1, T* smem_warp) {
+  using VT = typename Vec<T, V>::type;
+  static_assert(NPF >= 2, "the input ring needs at least the current and the next row");
+  constexpr int H = halo_lanes(V);
+  constexpr int kIn = 32 * V;
+  constexpr int kRow = NF * kIn;
+  const int lane = threadIdx.x & 31;
+  T* in_ring = smem_warp + lane * V;
+  T* xs_ring = in_ring + NPF * kRow;
+  const bool writer = lane >= H && lane < 32 - H;
+  const int mend = y1 + 2;
+
+  YPipe<T, V> yp;
+  yp.init();
+#pragma unroll
+  for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(xs_ring + 2 * kRow + k * kIn) = VT{};
+  const T* next = g.src + (long long)(y0 - 2) * g.pitch + xs + lane * V;  // next row to fetch
+#pragma unroll
+  for (int j = 0; j < NPF - 1; ++j) {
+    fetch_interior<T, V>(in_ring + j * kRow, next, g.plane);
+    next += g.pitch;
+  }
+  T* out = g.dst + (long long)y0 * g.pitch + xs + lane * V;  // next row written
+  int islot = 0, xslot = 0;
+  for (int m = y0 - 2; m < mend; ++m) {
+    if (m + NPF - 1 < mend) {
+      fetch_interior<T, V>(in_ring + (islot == 0 ? NPF - 1 : islot - 1) * kRow, next, g.plane);
+      next += g.pitch;
+    } else {
+      cp_async_commit();  // keep one group per row
+    }
+    cp_async_wait<NPF - 1>();
+    T f[NF][V];
+#pragma unroll
+    for (int k = 0; k < NF; ++k) unpack(*reinterpret_cast<const VT*>(in_ring + islot * kRow + k * kIn), f[k]);
+    sweep_x_lane<T, V>(f, c.x);
+    ring_left(yp, f, xs_ring, xslot, c.y);
+    if (m >= y0 + 2) {  // row m-2 is complete
+      T gf[NF][V];
+      ring_output(yp, gf, xs_ring, xslot, c.y);
+#pragma unroll
+      for (int k = 0; k < NF; ++k) store_if(writer, reinterpret_cast<VT*>(out + k * g.plane), pack(gf[k]));
+      out += g.pitch;
+    }
+    yp.right(c.y);
+    islot = islot + 1 == NPF ? 0 : islot + 1;
+    xslot = xslot == 2 ? 0 : xslot + 1;
+  }
+}
+
 // Producer warp: step A of strip `strip`, rows [y0, y1) of the tile, handing its rows to
 // the consumer; `u` counts the queue's handoffs (it continues across tiles).  A one_step
 // tile (an odd last step, or le_step_soa's far end, which g.far_rot selects) hands over

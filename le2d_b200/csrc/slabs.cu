@@ -56,9 +56,9 @@ struct Slab {
 };
 
 // Variant of each launch: FP32 two steps on warp pairs (one-step variant 2 for odd
-// remainders and SoA), FP64 one step (variant 0), as for whole tasks.
-int two_step_variant() { return sizeof(T) == 4 ? 13 : 0; }
-int one_step_variant() { return sizeof(T) == 4 ? 2 : 0; }
+// remainders and SoA), FP64 one step (variant 14), as for whole tasks.
+int two_step_variant() { return sizeof(T) == 4 ? 13 : 14; }
+int one_step_variant() { return sizeof(T) == 4 ? 2 : 14; }
 
 }  // namespace
 

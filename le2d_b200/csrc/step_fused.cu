@@ -69,17 +69,25 @@ __host__ __device__ constexpr int warp_elems() {
   return D == 2 ? march::warp_smem_elems2<T, V, NPF>() : march::warp_smem_elems<T, V, NPF>();
 }
 
-template <typename T, int V, int MINB, int NPF, int D>
+template <typename T, int V, int MINB, int NPF, int D, int F>
 __global__ void __launch_bounds__(kWarps * 32, MINB) fused_step_kernel(const FusedParams<T> p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int wib = threadIdx.x >> 5;
   const int task = blockIdx.x * kWarps + wib;
   if (task >= p.ntasks) return;  // whole warp leaves together
   T* smem = reinterpret_cast<T*>(smem_raw) + wib * warp_elems<T, V, NPF, D>();
-  const int strip = task % p.nstrips;
-  const int seg = task / p.nstrips;
+  int strip = task % p.nstrips;
+  int seg = task / p.nstrips;
+  if constexpr (F == 2) interior_first(p, task, strip, seg);
   const int y0 = seg * p.seg_len;
   const int y1 = min(y0 + p.seg_len, p.g.ny);
+  if constexpr (D == 1 && F >= 1) {  // interior tiles on the lean loop
+    const int xs = strip * strip_cols(V) - halo_lanes(V) * V;
+    if (march::tile_is_interior1<T, V>(p.g, xs, y0, y1)) {
+      march::march_tile_interior<T, V, NPF>(p.g, p.c, xs, y0, y1, smem);
+      return;
+    }
+  }
   if constexpr (D == 2)
     march::march_tile2<T, V, NPF, false>(p.g, p.c, strip, y0, y1, smem);
   else
@@ -156,6 +164,7 @@ template <> struct VariantCfg<float, 10> { static constexpr int V = 4, MINB = 3,
 template <> struct VariantCfg<float, 11> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 2, P = 1, W = 4, F = 1; };
 template <> struct VariantCfg<float, 12> { static constexpr int V = 4, MINB = 8, NPF = 2, D = 2, P = 1, W = 2, F = 1; };
 template <> struct VariantCfg<float, 13> { static constexpr int V = 4, MINB = 8, NPF = 2, D = 2, P = 1, W = 2, F = 2; };
+template <> struct VariantCfg<float, 14> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 1, P = 0, W = 4, F = 2; };
 template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
 template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
 template <> struct VariantCfg<double, 2> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
@@ -170,17 +179,19 @@ template <> struct VariantCfg<double, 10> { static constexpr int V = 2, MINB = 4
 template <> struct VariantCfg<double, 11> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 2, P = 1, W = 4, F = 1; };
 template <> struct VariantCfg<double, 12> { static constexpr int V = 2, MINB = 6, NPF = 2, D = 2, P = 1, W = 2, F = 1; };
 template <> struct VariantCfg<double, 13> { static constexpr int V = 2, MINB = 6, NPF = 2, D = 2, P = 1, W = 2, F = 2; };
-constexpr int kVariants = 14;
+template <> struct VariantCfg<double, 14> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 1, P = 0, W = 4, F = 2; };
+constexpr int kVariants = 15;
 
 template <typename T, int VAR>
 struct VariantKernel {
   using C = VariantCfg<T, VAR>;
-  static_assert(C::P == 1 || (C::F == 0 && C::W == kWarps), "lean loops and block size: warp pairs only");
+  static_assert(C::P == 1 || C::W == kWarps, "block size: warp pairs only");
+  static_assert(C::P == 1 || C::D == 1 || C::F == 0, "lean loops: warp pairs and one-step tiles");
   static void* fn() {
     if constexpr (C::P == 1)
       return (void*)fused_pair_kernel<T, C::V, C::MINB, C::NPF, C::W, C::F>;
     else
-      return (void*)fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D>;
+      return (void*)fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D, C::F>;
   }
   static size_t smem() {
     if constexpr (C::P == 1)
@@ -205,7 +216,7 @@ struct VariantKernel {
     if constexpr (C::P == 1)
       fused_pair_kernel<T, C::V, C::MINB, C::NPF, C::W, C::F><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
     else
-      fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
+      fused_step_kernel<T, C::V, C::MINB, C::NPF, C::D, C::F><<<pl.blocks, pl.threads, pl.smem, s>>>(p);
   }
 };
 
@@ -225,6 +236,7 @@ R with_variant(int var, A&&... a) {
     case 11: return Op<T, 11>::run(a...);
     case 12: return Op<T, 12>::run(a...);
     case 13: return Op<T, 13>::run(a...);
+    case 14: return Op<T, 14>::run(a...);
     default: return Op<T, 0>::run(a...);
   }
 }
@@ -340,13 +352,16 @@ cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pi
   p.c = c;
   p.yq = YPairs{};
   if constexpr (std::is_same<T, float>::value) p.yq = make_ypairs(c.y);
-  {  // the interior tiles' rectangle (tile_is_interior for two-step strips and segments)
-    const int V = plan.lanes, H = halo_lanes2(V) * V, out = strip_cols2(V), L = plan.seg_len;
+  {  // the interior tiles' rectangle (tile_is_interior / tile_is_interior1: the strip inside
+     // [0, nx), the rows read, 2 per step beyond the tile's, inside [0, ny))
+    const int V = plan.lanes, L = plan.seg_len, margin = 2 * plan.depth;
+    const int H = (plan.depth == 2 ? halo_lanes2(V) : halo_lanes(V)) * V;
+    const int out = plan.depth == 2 ? strip_cols2(V) : strip_cols(V);
     p.s_lo = (H + out - 1) / out;
     p.s_hi = nx - 32 * V + H >= 0 ? (nx - 32 * V + H) / out + 1 : 0;
     if (p.s_hi > plan.nstrips) p.s_hi = plan.nstrips;
-    p.g_lo = (4 + L - 1) / L;
-    p.g_hi = ny >= 4 ? (ny - 4) / L : 0;
+    p.g_lo = (margin + L - 1) / L;
+    p.g_hi = ny >= margin ? (ny - margin) / L : 0;
     if (p.s_hi < p.s_lo) p.s_hi = p.s_lo;
     if (p.g_hi < p.g_lo) p.g_hi = p.g_lo;
   }

@@ -244,19 +244,19 @@ def test_temporal_blocking_edges(libs, prec):
 
 @pytest.mark.parametrize("prec", ["f", "d"])
 def test_interior_tiles_lean_loops(libs, prec):
-    """Grids wide and tall enough that most two-step tiles are interior (strip inside the
-    grid, 4 rows of margin above and below), which the lean interior loops take, with even
-    and odd segment lengths: bitwise equal to one step per launch."""
+    """Grids wide and tall enough that most tiles are interior (strip inside the grid, 2 rows
+    of margin per step above and below), which the lean loops take, with even and odd
+    segment lengths: every variant, one or two steps per launch, bitwise equal to the first
+    one-step variant."""
     lib = libs[prec]
     vs = variants(lib)
-    two = [v for v, d in vs.items() if d == 2]
     one = [v for v, d in vs.items() if d == 1][0]
     rng = np.random.default_rng(23)
     for nx, ny, steps in ((517, 301, 10), (1000, 97, 7)):
         c = dict(nx=nx, ny=ny, hx=1.0, hy=0.9, c1=2.0, c2=1.1, rho=1.3, dt=0.2, stype=ST_AOS)
         g0 = rng.uniform(-1, 1, size=5 * nx * ny).astype(lib.dtype)
         ref = None
-        for var, seg in [(one, 0)] + [(v, s) for v in two for s in (0, 8, 9, 40)]:
+        for var, seg in [(one, 0)] + [(v, s) for v in sorted(vs) for s in (0, 8, 9, 40)]:
             t = make_task(lib, c)
             try:
                 assert lib.set_variant(t, var, seg) == 0
