@@ -91,25 +91,24 @@ __device__ __forceinline__ float ratio(float a, float b) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
   return a * r;
 }
-// FP64: Newton-Raphson division.  The hardware reciprocal estimate y0 (about 23 bits) is
-// refined by two Newton steps y <- y + y (1 - b y) (each doubles the correct bits), and the
-// quotient q = a y by one correction with its FMA residual, q + (a - b q) y (Markstein's
-// final step): within an ulp of the IEEE quotient, at about half the instructions of the
-// full division sequence.  Outside 2^-1022 <= |b| < 2^1022 (b = +-0, denormal, huge,
-// +-inf, NaN) the iteration breaks down, but the estimate is +-inf, 0 or NaN there and
-// a * y0 is the quotient's limit the limiter needs (+-inf / NaN for b = 0, 0 for huge or
-// infinite b); the choice is a select, not a branch (a branch per ratio costs more than the
-// division).
+// FP64: Newton-Raphson division.  The hardware reciprocal estimate y0 (relative error
+// around 2^-23) is refined by one Newton step y = y0 + y0 (1 - b y0) (error about its
+// square, 2^-46), and the quotient q = a y by one correction with its FMA residual,
+// r = q + (a - b q) y (Markstein's final step), whose error is of the order of the square
+// of y's (2^-92) before the final rounding: within an ulp of the IEEE quotient.  Outside
+// 2^-1022 <= |b| < 2^1022 (b = +-0, denormal, huge, +-inf, NaN) the iteration breaks down,
+// but the estimate is +-inf, 0 or NaN there and a * y0 is the quotient's limit the limiter
+// needs (+-inf / NaN for b = 0, 0 for huge or infinite b).  The range test reads b's
+// exponent field (1 <= e <= 2044) with integer operations, and the choice is a select,
+// not a branch (a branch per ratio costs more than the division).
 __device__ __forceinline__ double ratio(double a, double b) {
   double y0;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(b));
-  double y = fma(y0, fma(-b, y0, 1.0), y0);
-  y = fma(y, fma(-b, y, 1.0), y);
+  const double y = fma(y0, fma(-b, y0, 1.0), y0);
   const double q = a * y;
   const double r = fma(fma(-b, q, a), y, q);
-  const double ab = fabs(b);
-  const bool normal = (ab >= 0x1p-1022) & (ab < 0x1p+1022);  // & : no short-circuit branch
-  return normal ? r : a * y0;
+  const unsigned e = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
+  return e - 1u < 2044u ? r : a * y0;
 }
 
 __device__ __forceinline__ float max3(float a, float b, float c) {
@@ -119,19 +118,36 @@ __device__ __forceinline__ float max3(float a, float b, float c) {
 }
 __device__ __forceinline__ double max3(double a, double b, double c) { return fmax(a, fmax(b, c)); }
 
-// kc * superbee(r), superbee(r) = max(0, min(1, 2r), min(2, r))  (simple/le_core.c:38).
-// FP64: as written; fmin returns the non-NaN operand, so superbee(NaN) = max(0, 1, 2) = 2
-// as the reference's le_min/le_max give.  FP32: max(sat(2r), min(2, r)), the same
-// function with one min/max less -- sat clamps 2r to [0, 1] (so r <= 0 gives 0 from both
+// kc * superbee(r), superbee(r) = max(0, min(1, 2r), min(2, r))  (simple/le_core.c:38);
+// the reference's le_min/le_max give superbee(NaN) = max(0, 1, 2) = 2.  FP32:
+// max(sat(2r), min(2, r)), the same function with one min/max less -- sat clamps 2r to [0, 1] (so r <= 0 gives 0 from both
 // terms) and flushes NaN to 0, while min(2, NaN) = 2, keeping superbee(NaN) = 2.
 __device__ __forceinline__ float psi(float r, float kc) {
   return kc * fmaxf(__saturatef(r + r), fminf(2.0f, r));
 }
+// FP64 without floating-point compares: superbee(r) is one of 0, 2r, 1, r and 2, and which
+// one follows from r's high word h alone, because the breakpoints 0.5, 1 and 2 have zero low
+// words (so, for r >= 0, r < 1 <=> h < h(1), and so on): r in [1, 2) keeps r, below that 1,
+// from 2 on (with +inf and NaN) 2 -- a clamp of h to [h(1), h(2)] with the low word kept
+// only inside -- then 2r below 0.5 and 0 for negative r, and 2 for a NaN of either sign
+// (the GPU's 0 * inf, the ratio 0 / 0, has its sign bit set).  Equal to the reference's
+// le_max3(0, le_min(1, 2r), le_min(2, r)) for every r (a NaN is told by its high word:
+// magnitude above that of inf, true of every NaN arithmetic produces).
 __device__ __forceinline__ double psi(double r, double kc) {
-  // the two fmin results are never NaN, so the maxima are plain compare-selects
-  const double v = fmin(1.0, r + r), w = fmin(2.0, r);
-  const double m = v > w ? v : w;
-  return kc * (m > 0.0 ? m : 0.0);
+  constexpr int kH05 = 0x3fe00000, kH1 = 0x3ff00000, kH2 = 0x40000000;  // high words of 0.5, 1, 2
+  const int h = __double2hiint(r), l = __double2loint(r);
+  int ho = min(max(h, kH1), kH2);
+  int lo = h >= kH1 && h < kH2 ? l : 0;
+  const double r2 = r + r;
+  if (h < kH05) {  // 0 <= r < 0.5: 2r; r < 0: 0 (selects, not a branch)
+    ho = h < 0 ? 0 : __double2hiint(r2);
+    lo = h < 0 ? 0 : __double2loint(r2);
+  }
+  if ((h & 0x7fffffff) > 0x7ff00000) {  // NaN
+    ho = kH2;
+    lo = 0;
+  }
+  return kc * __hiloint2double(ho, lo);
 }
 
 // Differences of the four moving invariants across a face, formed from the differences

@@ -274,6 +274,47 @@ def test_interior_tiles_lean_loops(libs, prec):
 
 
 @pytest.mark.parametrize("prec", ["f", "d"])
+def test_zero_divisor_slope_ratios(libs, prec):
+    """One velocity component whose neighbours differ by exactly -eps or +eps (all else zero),
+    so that P = D + eps or Q = eps - D is exactly 0 at many faces: slope ratios x/0 (+-inf)
+    and 0/0 (NaN) reach the limiter, where superbee(+inf) = superbee(NaN) = 2 and
+    superbee(-inf) = 0 as in the reference.  Every variant against the oracle, one to three
+    steps (two-step variants take the second and third on warp pairs).  (With both components set, the y-sweep meets faces where D = -eps holds in the
+    reference's invariant differences but not, by one rounding, in the field differences the
+    kernels form, or the reverse: such exact ties can take either limiter branch, so that case
+    compares two schemes' roundings rather than the division.)"""
+    lib = libs[prec]
+    o = Oracle(prec)
+    nx, ny = 260, 150
+    rng = np.random.default_rng(31)
+    eps = np.array(1e-6, dtype=o.dtype)
+    # material and steps chosen so that, after the first step, fields are no longer small
+    # dyadic multiples of eps (exact ties, see above, then become improbable)
+    c = dict(nx=nx, ny=ny, hx=0.97, hy=1.03, c1=2.1, c2=1.13, rho=1.37, dt=0.21, stype=ST_AOS)
+    for field, sign in ((0, 1), (1, -1)):  # vx in {0, eps}; vy in {0, -eps}
+        g0 = np.zeros(5 * nx * ny, dtype=o.dtype)
+        g0[field::5] = sign * rng.integers(0, 2, size=nx * ny).astype(o.dtype) * eps
+        for steps in (1, 2, 3):
+            want = g0.copy()
+            o.run(want, nx, ny, c["dt"], c["hx"], c["hy"], c["c1"], c["c2"], c["rho"], ST_AOS, steps)
+            gd = g0.astype(np.float64)
+            Oracle("d").run(gd, nx, ny, c["dt"], c["hx"], c["hy"], c["c1"], c["c2"], c["rho"], ST_AOS, steps)
+            for var in sorted(variants(lib)):
+                t = make_task(lib, c)
+                try:
+                    assert lib.set_variant(t, var, 16) == 0
+                    assert lib.upload(t, g0.copy()) == 0
+                    assert lib.step_n(t, steps) == 0
+                    got = np.zeros_like(g0)
+                    assert lib.download(t, got) == 0
+                    assert lib.last_error(t) == 0
+                finally:
+                    lib.le_free_task(t)
+                assert np.all(np.isfinite(got)), (field, var, steps)
+                check(prec, got, want, gd, nx, ny, ST_AOS, f"zero-divisor/{prec}/f{field}/v{var}/{steps}")
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
 def test_uniform_state_is_fixed_point(libs, prec):
     c = dict(nx=257, ny=131, hx=1.0, hy=1.0, c1=2.0, c2=1.0, rho=1.0, dt=0.25, stype=ST_AOS)
     g0 = np.tile(np.array([0.3, -0.2, 1.5, 0.25, -0.7], libs[prec].dtype), 257 * 131)
