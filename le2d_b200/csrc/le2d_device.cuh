@@ -136,17 +136,15 @@ __device__ __forceinline__ float psi(float r, float kc) {
 __device__ __forceinline__ double psi(double r, double kc) {
   constexpr int kH05 = 0x3fe00000, kH1 = 0x3ff00000, kH2 = 0x40000000;  // high words of 0.5, 1, 2
   const int h = __double2hiint(r), l = __double2loint(r);
+  const double r2 = r + r;
+  const bool small = h < kH05, neg = h < 0, nan = (h & 0x7fffffff) > 0x7ff00000;
+  // written as selects: a branch here would diverge within the warp
   int ho = min(max(h, kH1), kH2);
   int lo = h >= kH1 && h < kH2 ? l : 0;
-  const double r2 = r + r;
-  if (h < kH05) {  // 0 <= r < 0.5: 2r; r < 0: 0 (selects, not a branch)
-    ho = h < 0 ? 0 : __double2hiint(r2);
-    lo = h < 0 ? 0 : __double2loint(r2);
-  }
-  if ((h & 0x7fffffff) > 0x7ff00000) {  // NaN
-    ho = kH2;
-    lo = 0;
-  }
+  ho = small ? (neg ? 0 : __double2hiint(r2)) : ho;  // 0 <= r < 0.5: 2r; r < 0: 0
+  lo = small ? (neg ? 0 : __double2loint(r2)) : lo;
+  ho = nan ? kH2 : ho;
+  lo = nan ? 0 : lo;
   return kc * __hiloint2double(ho, lo);
 }
 
