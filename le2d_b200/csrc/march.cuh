@@ -181,6 +181,30 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Stores of one lane's V columns that only the lanes with `p` set perform (a predicated
+// store, not a branch around it).
+__device__ __forceinline__ void store_if(bool p, float4* a, const float4& v) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.v4.f32 [%1], {%2, %3, %4, %5};\n\t}" ::"r"(
+          (unsigned)p),
+      "l"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w));
+}
+__device__ __forceinline__ void store_if(bool p, float2* a, const float2& v) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.v2.f32 [%1], {%2, %3};\n\t}" ::"r"(
+                   (unsigned)p),
+               "l"(a), "f"(v.x), "f"(v.y));
+}
+__device__ __forceinline__ void store_if(bool p, double2* a, const double2& v) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.v2.f64 [%1], {%2, %3};\n\t}" ::"r"(
+                   (unsigned)p),
+               "l"(a), "d"(v.x), "d"(v.y));
+}
+__device__ __forceinline__ void store_if(bool p, double* a, const double& v) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.f64 [%1], %2;\n\t}" ::"r"(
+                   (unsigned)p),
+               "l"(a), "d"(v));
+}
+
 // Starts copying source row `row` into this lane's slot of the input ring.  Strips that
 // reach past the grid edge load their clamped columns synchronously instead.
 template <typename T, int V, bool COHERENT>
@@ -458,14 +482,12 @@ __device__ __forceinline__ void march_tile(const GridRef<T>& g, const StepConsts
 #pragma unroll
       for (int k = 0; k < NF; ++k) unpack(*reinterpret_cast<const VT*>(rg + k * kIn), gf[k]);
       yp.apply(gf, cy);
-      if (writer) {
-        T* out = g.dst + (long long)row * g.pitch + col0;
+      T* out = g.dst + (long long)row * g.pitch + col0;
 #pragma unroll
-        for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(out + k * g.plane) = pack(gf[k]);
-        if (TAP && row == tap.row) {
-          *reinterpret_cast<VT*>(tap.out + col0) = pack(gf[VX]);
-          *reinterpret_cast<VT*>(tap.out + g.pitch + col0) = pack(gf[VY]);
-        }
+      for (int k = 0; k < NF; ++k) store_if(writer, reinterpret_cast<VT*>(out + k * g.plane), pack(gf[k]));
+      if (TAP && row == tap.row && writer) {
+        *reinterpret_cast<VT*>(tap.out + col0) = pack(gf[VX]);
+        *reinterpret_cast<VT*>(tap.out + g.pitch + col0) = pack(gf[VY]);
       }
     }
 

@@ -133,30 +133,6 @@ __device__ __forceinline__ void tap_row(const RowTap<T>& tap, long long pitch, i
   *reinterpret_cast<VT*>(tap.out + pitch + col0) = pack(f[VY]);
 }
 
-// Stores of one lane's V columns that only the lanes with `p` set perform (a predicated
-// store, not a branch around it).
-__device__ __forceinline__ void store_if(bool p, float4* a, const float4& v) {
-  asm volatile(
-      "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.v4.f32 [%1], {%2, %3, %4, %5};\n\t}" ::"r"(
-          (unsigned)p),
-      "l"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w));
-}
-__device__ __forceinline__ void store_if(bool p, float2* a, const float2& v) {
-  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.v2.f32 [%1], {%2, %3};\n\t}" ::"r"(
-                   (unsigned)p),
-               "l"(a), "f"(v.x), "f"(v.y));
-}
-__device__ __forceinline__ void store_if(bool p, double2* a, const double2& v) {
-  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.v2.f64 [%1], {%2, %3};\n\t}" ::"r"(
-                   (unsigned)p),
-               "l"(a), "d"(v.x), "d"(v.y));
-}
-__device__ __forceinline__ void store_if(bool p, double* a, const double& v) {
-  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.f64 [%1], %2;\n\t}" ::"r"(
-                   (unsigned)p),
-               "l"(a), "d"(v));
-}
-
 // Interior tiles.  When the strip lies inside [0, nx), every row the tile reads lies inside
 // [0, ny) (y0 >= 4, y1 + 4 <= ny) and the tile takes two steps, no column or row is
 // clamped and every step-A row ka in [y0-2, y1+2) is handed over exactly once -- the same
@@ -482,11 +458,9 @@ __device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepCons
 #pragma unroll
       for (int k = 0; k < NF; ++k) unpack(*reinterpret_cast<const VT*>(slot + k * kIn), fa[k]);
       mbar_arrive(empty + hs);
-      if (writer) {
-        T* out = g.dst + (long long)ka * g.pitch + col0;
+      T* out = g.dst + (long long)ka * g.pitch + col0;
 #pragma unroll
-        for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(out + k * g.plane) = pack(fa[k]);
-      }
+      for (int k = 0; k < NF; ++k) store_if(writer, reinterpret_cast<VT*>(out + k * g.plane), pack(fa[k]));
       ++u;
       continue;
     }
@@ -500,13 +474,11 @@ __device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepCons
       if (bin >= y0 + 2) {  // step-B row bin-2 is complete
         T gb[NF][V];
         ring_output(yb, gb, b_ring, bslot, c.y);
-        if (writer) {
-          const int row = bin - 2;
-          T* out = g.dst + (long long)row * g.pitch + col0;
+        const int row = bin - 2;
+        T* out = g.dst + (long long)row * g.pitch + col0;
 #pragma unroll
-          for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(out + k * g.plane) = pack(gb[k]);
-          if (TAP && row == tap_b.row) tap_row<T, V>(tap_b, g.pitch, col0, gb);
-        }
+        for (int k = 0; k < NF; ++k) store_if(writer, reinterpret_cast<VT*>(out + k * g.plane), pack(gb[k]));
+        if (TAP && row == tap_b.row && writer) tap_row<T, V>(tap_b, g.pitch, col0, gb);
       }
       yb.right(c.y);
       bslot = bslot == 2 ? 0 : bslot + 1;
