@@ -30,7 +30,7 @@
 namespace le2d {
 namespace march {
 
-constexpr int kHand = 2;  // queue slots between the warps of a pair
+constexpr int kHand = 1;  // queue slots between the warps of a pair
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return (unsigned)__cvta_generic_to_shared(p);
