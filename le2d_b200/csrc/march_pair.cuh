@@ -138,10 +138,10 @@ __device__ __forceinline__ void tap_row(const RowTap<T>& tap, long long pitch, i
 // clamped and every step-A row ka in [y0-2, y1+2) is handed over exactly once -- the same
 // handoffs pair_produce / pair_consume make for such a tile, in the same order.  These
 // loops drop the clamps and the per-row use counts, step the row addresses instead of
-// recomputing them and store with predicates: about 8 % fewer instructions per node-update
+// recomputing them and store with predicates: about 9 % fewer instructions per node-update
 // with a loop no larger than the general one (a loop over two rows, which would let the
 // y-pipeline's replaced states alternate instead of being copied, measured slower: it no
-// longer fits the instruction cache).
+// longer fits the instruction cache).  Any input-ring depth NPF >= 2.
 template <typename T, int V>
 __device__ __forceinline__ bool tile_is_interior(const GridRef<T>& g, int xs, int y0, int y1) {
   return xs >= 0 && xs + 32 * V <= g.nx && y0 >= 4 && y1 + 4 <= g.ny;
