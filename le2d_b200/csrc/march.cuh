@@ -182,27 +182,32 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // Stores of one lane's V columns that only the lanes with `p` set perform (a predicated
-// store, not a branch around it).
+// store, not a branch around it).  Memory clobbers keep them ordered with the fences and
+// release stores that publish a tile in the batched kernel.
 __device__ __forceinline__ void store_if(bool p, float4* a, const float4& v) {
   asm volatile(
       "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.v4.f32 [%1], {%2, %3, %4, %5};\n\t}" ::"r"(
           (unsigned)p),
-      "l"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w));
+      "l"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+      : "memory");
 }
 __device__ __forceinline__ void store_if(bool p, float2* a, const float2& v) {
   asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.v2.f32 [%1], {%2, %3};\n\t}" ::"r"(
                    (unsigned)p),
-               "l"(a), "f"(v.x), "f"(v.y));
+               "l"(a), "f"(v.x), "f"(v.y)
+               : "memory");
 }
 __device__ __forceinline__ void store_if(bool p, double2* a, const double2& v) {
   asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.v2.f64 [%1], {%2, %3};\n\t}" ::"r"(
                    (unsigned)p),
-               "l"(a), "d"(v.x), "d"(v.y));
+               "l"(a), "d"(v.x), "d"(v.y)
+               : "memory");
 }
 __device__ __forceinline__ void store_if(bool p, double* a, const double& v) {
   asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.f64 [%1], %2;\n\t}" ::"r"(
                    (unsigned)p),
-               "l"(a), "d"(v));
+               "l"(a), "d"(v)
+               : "memory");
 }
 
 // Starts copying source row `row` into this lane's slot of the input ring.  Strips that
