@@ -129,10 +129,10 @@ __device__ __forceinline__ float psi(float r, float kc) {
 // one follows from r's high word h alone, because the breakpoints 0.5, 1 and 2 have zero low
 // words (so, for r >= 0, r < 1 <=> h < h(1), and so on): r in [1, 2) keeps r, below that 1,
 // from 2 on (with +inf and NaN) 2 -- a clamp of h to [h(1), h(2)] with the low word kept
-// only inside -- then 2r below 0.5 and 0 for negative r, and 2 for a NaN of either sign
-// (the GPU's 0 * inf, the ratio 0 / 0, has its sign bit set).  Equal to the reference's
-// le_max3(0, le_min(1, 2r), le_min(2, r)) for every r (a NaN is told by its high word:
-// magnitude above that of inf, true of every NaN arithmetic produces).
+// only inside -- then 2r below 0.5, 0 for negative r, and 2 for a NaN of either sign (the
+// ratio 0 / 0).  Equal to the reference's le_max3(0, le_min(1, 2r), le_min(2, r)) for every
+// r (a NaN is told by its high word: magnitude above that of inf, which holds for every
+// quiet NaN and so for every NaN arithmetic produces).
 __device__ __forceinline__ double psi(double r, double kc) {
   constexpr int kH05 = 0x3fe00000, kH1 = 0x3ff00000, kH2 = 0x40000000;  // high words of 0.5, 1, 2
   const int h = __double2hiint(r), l = __double2loint(r);
