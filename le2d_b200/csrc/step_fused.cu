@@ -165,6 +165,7 @@ template <> struct VariantCfg<float, 11> { static constexpr int V = 4, MINB = 4,
 template <> struct VariantCfg<float, 12> { static constexpr int V = 4, MINB = 8, NPF = 2, D = 2, P = 1, W = 2, F = 1; };
 template <> struct VariantCfg<float, 13> { static constexpr int V = 4, MINB = 8, NPF = 2, D = 2, P = 1, W = 2, F = 2; };
 template <> struct VariantCfg<float, 14> { static constexpr int V = 4, MINB = 4, NPF = 2, D = 1, P = 0, W = 4, F = 2; };
+template <> struct VariantCfg<float, 15> { static constexpr int V = 4, MINB = 5, NPF = 2, D = 1, P = 0, W = 4, F = 2; };
 template <> struct VariantCfg<double, 0> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
 template <> struct VariantCfg<double, 1> { static constexpr int V = 2, MINB = 3, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
 template <> struct VariantCfg<double, 2> { static constexpr int V = 1, MINB = 4, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
@@ -180,7 +181,8 @@ template <> struct VariantCfg<double, 11> { static constexpr int V = 2, MINB = 3
 template <> struct VariantCfg<double, 12> { static constexpr int V = 2, MINB = 6, NPF = 2, D = 2, P = 1, W = 2, F = 1; };
 template <> struct VariantCfg<double, 13> { static constexpr int V = 2, MINB = 6, NPF = 2, D = 2, P = 1, W = 2, F = 2; };
 template <> struct VariantCfg<double, 14> { static constexpr int V = 2, MINB = 2, NPF = 2, D = 1, P = 0, W = 4, F = 2; };
-constexpr int kVariants = 15;
+template <> struct VariantCfg<double, 15> { static constexpr int V = 2, MINB = 4, NPF = 2, D = 1, P = 0, W = 4, F = 2; };
+constexpr int kVariants = 16;
 
 template <typename T, int VAR>
 struct VariantKernel {
@@ -237,6 +239,7 @@ R with_variant(int var, A&&... a) {
     case 12: return Op<T, 12>::run(a...);
     case 13: return Op<T, 13>::run(a...);
     case 14: return Op<T, 14>::run(a...);
+    case 15: return Op<T, 15>::run(a...);
     default: return Op<T, 0>::run(a...);
   }
 }
