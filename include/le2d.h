@@ -220,6 +220,13 @@ int le2d_device_layout(const le_task *task, long long *pitch_elems, long long *p
 /* Bytes of device memory a task of this size holds (for admission control). */
 size_t le2d_task_device_bytes(int nx, int ny);
 
+/* Self-test of the step kernels' FP64 slope-ratio division: for i < n, fast[i] = the
+ * kernels' a[i] / b[i] (a hardware reciprocal estimate, one Newton step and a Markstein
+ * correction) and ieee[i] = the correctly rounded quotient, both computed on the current
+ * device from host arrays.  New surface with no counterpart in the reference (whose
+ * division is the compiler's). */
+int le2d_selftest_ratio(const double *a, const double *b, long long n, double *fast, double *ieee);
+
 /* ---- One grid over several devices (row slabs) ---------------------------------------
  * The reference's multi-GPU step (cuda5/cuda6 le_core.cu:374-509: one process, row slabs,
  * peer copies of the rows next to each cut).  The task's grid (its size, dt, h, material

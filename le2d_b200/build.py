@@ -24,7 +24,7 @@ LIBDIR = os.path.join(PKG, "lib")
 INCLUDE = os.path.join(ROOT, "include")
 
 SOURCES = ["le2d_api.cu", "step_fused.cu", "step_split.cu", "layout.cu", "diag.cu", "batch.cu", "engine.cu",
-           "serve.cu", "diag_noalloc.cu", "slabs.cu"]
+           "serve.cu", "diag_noalloc.cu", "slabs.cu", "selftest.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -48,7 +48,7 @@ EXPORTS = [
     "le2d_server_stats", "le2d_now", "le2d_diagnostics_noalloc", "le2d_autotune", "le2d_autotune_reset",
     "le2d_batch_autotune", "le2d_batch_autotune_reset",
     "le2d_slabs_create", "le2d_slabs_destroy", "le2d_slabs_rows", "le2d_slabs_upload",
-    "le2d_slabs_download", "le2d_slabs_step_n", "le2d_slabs_wait",
+    "le2d_slabs_download", "le2d_slabs_step_n", "le2d_slabs_wait", "le2d_selftest_ratio",
 ]
 
 LE2D_DIAG_NOALLOC_MAX_ROWS = 16384
@@ -192,6 +192,8 @@ class Lib:
         L.le2d_slabs_download.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.le2d_slabs_step_n.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.le2d_slabs_wait.argtypes = [ctypes.c_void_p]
+        L.le2d_selftest_ratio.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
+                                          ctypes.c_void_p, ctypes.c_void_p]
         L.le2d_diagnostics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
                                                ctypes.c_longlong, R, R, R, R, R, ctypes.c_void_p,
                                                P(self.le2d_diag_t)]
@@ -297,6 +299,18 @@ class Lib:
 
     def batch_autotune_reset(self) -> int:
         return self.lib.le2d_batch_autotune_reset()
+
+    def selftest_ratio(self, a: np.ndarray, b: np.ndarray):
+        """The step kernels' FP64 slope-ratio division and IEEE division of a / b, on the device."""
+        a = np.ascontiguousarray(a, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        assert a.shape == b.shape and a.ndim == 1
+        fast, ieee = np.empty_like(a), np.empty_like(a)
+        rc = self.lib.le2d_selftest_ratio(a.ctypes.data, b.ctypes.data, a.size, fast.ctypes.data,
+                                          ieee.ctypes.data)
+        if rc:
+            raise RuntimeError(self.strerror(rc))
+        return fast, ieee
 
     def sim_time(self, t):
         tt, st = ctypes.c_double(0.0), ctypes.c_longlong(0)

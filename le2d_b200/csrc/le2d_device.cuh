@@ -16,7 +16,12 @@
 //       G_i = u_i - psi'_i D_{i-1}, psi'_i = psi(Q_i / Q_{i-1}), new u_i = u_i - k (G_i - G_{i+1})
 // with psi(r) = (1 - k)/2 * superbee(r).
 //
-// Difference form.  The flux differences need only the face differences D:
+// FP64 computes exactly these expressions in the reference's operation order, each
+// operation rounded once as the reference double build rounds it (namespace ex), so its
+// results are the reference's bit for bit: which faces see an exact tie P = 0 (D = -eps)
+// depends on every rounding of the sweep before, and there the limiter jumps.
+//
+// FP32: difference form.  The flux differences need only the face differences D:
 //   A_i = F_{i-1} - F_i = t_{i-1} - psi_i D_i,        t_i = (psi_i - 1) D_i
 //   B_i = G_{i+1} - G_i = c_i - psi'_{i+1} D_i,       c_i = D_i + psi'_i D_{i-1}
 // and D itself is formed from differences of the fields (face_differences), so the
@@ -95,20 +100,25 @@ __device__ __forceinline__ float ratio(float a, float b) {
 // around 2^-23) is refined by one Newton step y = y0 + y0 (1 - b y0) (error about its
 // square, 2^-46), and the quotient q = a y by one correction with its FMA residual,
 // r = q + (a - b q) y (Markstein's final step), whose error is of the order of the square
-// of y's (2^-92) before the final rounding: within an ulp of the IEEE quotient.  Outside
-// 2^-1022 <= |b| < 2^1022 (b = +-0, denormal, huge, +-inf, NaN) the iteration breaks down,
-// but the estimate is +-inf, 0 or NaN there and a * y0 is the quotient's limit the limiter
-// needs (+-inf / NaN for b = 0, 0 for huge or infinite b).  The range test reads b's
-// exponent field (1 <= e <= 2044) with integer operations, and the choice is a select,
-// not a branch (a branch per ratio costs more than the division).
+// of y's (2^-92) before the final rounding.  So r is the correctly rounded quotient unless
+// a / b lies within about 2^-92 (relative) of a midpoint between two doubles -- on random
+// operands about one division in 2^39; tests/test_division_gpu.py compares it with IEEE
+// division.  The slope ratios have the form a = D' + eps, b = D + eps (or eps - D), so b is
+// +0 exactly at a tie (D = -eps, never -0 under round-to-nearest) and otherwise at least
+// 2^-73 in magnitude (the exact difference of two doubles near eps).  For b = 0 the
+// division gives +inf (a > 0), -inf (a < 0) or NaN (a = 0), which the limiter maps to 2,
+// 0 and 2: the select returns copysign(inf, a), which the limiter maps the same way (a is
+// never -0 either).  Outside the supported range: magnitudes of 2^1022 and above (state
+// values near overflow) and operands below about 2^-970, where the residual underflows.
+// A select, not a branch: a branch per ratio costs more than the division.
 __device__ __forceinline__ double ratio(double a, double b) {
   double y0;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(b));
   const double y = fma(y0, fma(-b, y0, 1.0), y0);
   const double q = a * y;
   const double r = fma(fma(-b, q, a), y, q);
-  const unsigned e = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
-  return e - 1u < 2044u ? r : a * y0;
+  const double inf = __hiloint2double((__double2hiint(a) & (int)0x80000000) | 0x7ff00000, 0);
+  return b == 0.0 ? inf : r;
 }
 
 __device__ __forceinline__ float max3(float a, float b, float c) {
@@ -128,25 +138,70 @@ __device__ __forceinline__ float psi(float r, float kc) {
 // FP64 without floating-point compares: superbee(r) is one of 0, 2r, 1, r and 2, and which
 // one follows from r's high word h alone, because the breakpoints 0.5, 1 and 2 have zero low
 // words (so, for r >= 0, r < 1 <=> h < h(1), and so on): r in [1, 2) keeps r, below that 1,
-// from 2 on (with +inf and NaN) 2 -- a clamp of h to [h(1), h(2)] with the low word kept
-// only inside -- then 2r below 0.5, 0 for negative r, and 2 for a NaN of either sign (the
-// ratio 0 / 0).  Equal to the reference's le_max3(0, le_min(1, 2r), le_min(2, r)) for every
-// r (a NaN is told by its high word: magnitude above that of inf, which holds for every
-// quiet NaN and so for every NaN arithmetic produces).
+// from 2 on (with +inf) 2 -- a clamp of h to [h(1), h(2)] with the low word kept only
+// inside -- then 2r below 0.5 and 0 for negative r.  The FP64 ratio never returns NaN (a tie
+// gives copysign(inf, a), see ratio(double)); a positive NaN would land on 2 like the
+// reference's superbee(NaN).  The product kc * superbee(r), kc = (1 - k) / 2, rounds like
+// the reference's `limiter(r) / 2.0 * (1.0 - c)`: halving is exact.  The reference returns
+// -0 for r = -0 where this gives +0 (the same number).
 __device__ __forceinline__ double psi(double r, double kc) {
   constexpr int kH05 = 0x3fe00000, kH1 = 0x3ff00000, kH2 = 0x40000000;  // high words of 0.5, 1, 2
   const int h = __double2hiint(r), l = __double2loint(r);
   const double r2 = r + r;
-  const bool small = h < kH05, neg = h < 0, nan = (h & 0x7fffffff) > 0x7ff00000;
+  const bool small = h < kH05, neg = h < 0;
   // written as selects: a branch here would diverge within the warp
   int ho = min(max(h, kH1), kH2);
   int lo = h >= kH1 && h < kH2 ? l : 0;
   ho = small ? (neg ? 0 : __double2hiint(r2)) : ho;  // 0 <= r < 0.5: 2r; r < 0: 0
   lo = small ? (neg ? 0 : __double2loint(r2)) : lo;
-  ho = nan ? kH2 : ho;
-  lo = nan ? 0 : lo;
   return kc * __hiloint2double(ho, lo);
 }
+
+// Uncontracted FP64 arithmetic: each operation rounds once, as the reference's double
+// build computes (x86-64 baseline code, no fused multiply-add).  The compiler never fuses
+// these intrinsics.
+namespace ex {
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+
+// omega_x / omega_y (simple/le_core.c:192-218) in the reference's operation order:
+// n00 = sn * irhoc1, n01 = sxy * irhoc2, w = v -+ n.
+__device__ __forceinline__ void invariants(double vn, double sn, double vt, double sxy,
+                                           const Sweep<double>& c, double (&w)[4]) {
+  const double n00 = mul(sn, c.irhoc1), n01 = mul(sxy, c.irhoc2);
+  w[0] = sub(vn, n00);
+  w[1] = add(vn, n00);
+  w[2] = sub(vt, n01);
+  w[3] = add(vt, n01);
+}
+
+// The tail of tvd2 (simple/le_core.c:66-68) and reconstruct (:251-257) for one invariant
+// u: given the flux difference df = f12 - f_12, the change tvd2(...) - u.
+__device__ __forceinline__ double change(double u, double k, double df) {
+  return sub(sub(u, mul(k, df)), u);
+}
+
+// inc_x / inc_y (simple/le_core.c:221-249) from the four invariant changes, operation by
+// operation: d = 0.5 * change, vn += d1 + d2, vt += d3 + d4, sn += (d2 - d1) * rhoc1,
+// so += (d2 - d1) * rhoc3, sxy += rhoc2 * (d4 - d3).
+template <int AXIS>
+__device__ __forceinline__ void increment(double& vx, double& vy, double& sxx, double& sxy,
+                                          double& syy, double c1, double c2, double c3, double c4,
+                                          const Sweep<double>& c) {
+  double& vn = AXIS == 0 ? vx : vy;
+  double& vt = AXIS == 0 ? vy : vx;
+  double& sn = AXIS == 0 ? sxx : syy;
+  double& so = AXIS == 0 ? syy : sxx;
+  const double d1 = mul(0.5, c1), d2 = mul(0.5, c2), d3 = mul(0.5, c3), d4 = mul(0.5, c4);
+  const double p = sub(d2, d1);
+  vn = add(vn, add(d1, d2));
+  vt = add(vt, add(d3, d4));
+  sn = add(sn, mul(p, c.rhoc1));
+  so = add(so, mul(p, c.rhoc3));
+  sxy = add(sxy, mul(c.rhoc2, sub(d4, d3)));
+}
+}  // namespace ex
 
 // Differences of the four moving invariants across a face, formed from the differences
 // of the fields that enter them (normal velocity vn, normal stress sn, tangential

@@ -95,11 +95,78 @@ __device__ __forceinline__ void load_row(T (&f)[NF][V], const GridRef<T>& g, int
   }
 }
 
-// x-sweep of the V nodes of this lane (row in registers, neighbours by shuffles).
-// Face e (0..V) lies between node e-1 and node e of the lane; the neighbour lanes supply
-// the fields of nodes -1 and V and the flux terms of their edge nodes.
+// FP64 x-sweep in the reference's flux form (tvd2, simple/le_core.c:48-69): invariants
+// w of each node, face differences D = w_{i+1} - w_i, slope ratios, limited fluxes
+// F_i = w_i + psi_i D_i (right-moving w1, w3) and G_i = w_i - psi'_i D_{i-1} (left-moving
+// w2, w4), then u - k (f12 - f_12) - u and inc_x, every operation rounded as the reference
+// rounds it, so the result is the reference double build's bit for bit (up to the sign of
+// zero and the division's rounding, see ratio(double)).  Face e (0..V) of the lane lies
+// between its nodes e-1 and e; the neighbour lanes supply the invariants of nodes -1 and V
+// and the fluxes of their edge nodes.
+template <int V>
+__device__ __forceinline__ void sweep_x_lane_exact(double (&f)[NF][V], const Sweep<double>& c) {
+  constexpr unsigned kAll = 0xffffffffu;
+  const double eps = tvd_eps<double>();
+  double w[4][V + 2];  // nodes -1 .. V
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    double wv[4];
+    ex::invariants(f[VX][v], f[SXX][v], f[VY][v], f[SXY][v], c, wv);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) w[k][v + 1] = wv[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    w[k][0] = __shfl_up_sync(kAll, w[k][V], 1);
+    w[k][V + 1] = __shfl_down_sync(kAll, w[k][1], 1);
+  }
+  double dw[4][V];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const double kc = q ? c.kc2 : c.kc1;
+    const double kk = q ? c.k2 : c.k1;
+    {  // right-moving invariant (w1 / w3): psi_v = psi(P_left / P_right), F_v
+      const int k = 2 * q;
+      double d[V + 1], fl[V];
+#pragma unroll
+      for (int e = 0; e <= V; ++e) d[e] = ex::sub(w[k][e + 1], w[k][e]);
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const double ps = psi(ratio(ex::add(d[v], eps), ex::add(d[v + 1], eps)), kc);
+        fl[v] = ex::add(w[k][v + 1], ex::mul(ps, d[v + 1]));
+      }
+      const double f_in = __shfl_up_sync(kAll, fl[V - 1], 1);
+#pragma unroll
+      for (int v = 0; v < V; ++v) dw[k][v] = ex::change(w[k][v + 1], kk, ex::sub(fl[v], v ? fl[v - 1] : f_in));
+    }
+    {  // left-moving invariant (w2 / w4): psi'_v = psi(Q_right / Q_left), G_v
+      const int k = 2 * q + 1;
+      double d[V + 1], gl[V];
+#pragma unroll
+      for (int e = 0; e <= V; ++e) d[e] = ex::sub(w[k][e + 1], w[k][e]);
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const double ps = psi(ratio(ex::sub(eps, d[v + 1]), ex::sub(eps, d[v])), kc);
+        gl[v] = ex::sub(w[k][v + 1], ex::mul(ps, d[v]));
+      }
+      const double g_in = __shfl_down_sync(kAll, gl[0], 1);
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        dw[k][v] = ex::change(w[k][v + 1], kk, ex::sub(gl[v], v < V - 1 ? gl[v + 1] : g_in));
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < V; ++v)
+    ex::increment<0>(f[VX][v], f[VY][v], f[SXX][v], f[SXY][v], f[SYY][v], dw[0][v], dw[1][v],
+                     dw[2][v], dw[3][v], c);
+}
+
+// FP32 x-sweep of the V nodes of this lane in the difference form (row in registers,
+// neighbours by shuffles).  Face e (0..V) lies between node e-1 and node e of the lane;
+// the neighbour lanes supply the fields of nodes -1 and V and the flux terms of their
+// edge nodes.
 template <typename T, int V>
-__device__ __forceinline__ void sweep_x_lane(T (&f)[NF][V], const Sweep<T>& c) {
+__device__ __forceinline__ void sweep_x_lane_diff(T (&f)[NF][V], const Sweep<T>& c) {
   constexpr unsigned kAll = 0xffffffffu;
   const T eps = tvd_eps<T>();
   // fields entering the x-invariants: vn = vx, sn = sxx, vt = vy, and sxy
@@ -155,6 +222,16 @@ __device__ __forceinline__ void sweep_x_lane(T (&f)[NF][V], const Sweep<T>& c) {
   for (int v = 0; v < V; ++v)
     apply_increment<0>(f[VX][v], f[VY][v], f[SXX][v], f[SXY][v], f[SYY][v], a[0][v], b[0][v],
                        a[1][v], b[1][v], c);
+}
+
+// x-sweep of one lane's V nodes: FP32 in the difference form, FP64 in the reference's
+// flux form.
+template <typename T, int V>
+__device__ __forceinline__ void sweep_x_lane(T (&f)[NF][V], const Sweep<T>& c) {
+  if constexpr (sizeof(T) == 8)
+    sweep_x_lane_exact<V>(f, c);
+  else
+    sweep_x_lane_diff<T, V>(f, c);
 }
 
 // Shared memory of one warp: NPF rows of raw input (filled by cp.async, NPF-1 rows ahead)
@@ -231,65 +308,83 @@ __device__ __forceinline__ void fetch_row(T* slot, const GridRef<T>& g, int row,
   cp_async_commit();
 }
 
-// The per-column y-pipeline.  Row m arrives x-swept; with the fields of row m-1 it gives
-// the face differences D_{m-1}.  left() advances the left-moving invariants (B_{m-2},
-// c_{m-1}), apply() adds the increments of row m-2 to its fields, right() advances the
-// right-moving ones (A_{m-1}, t_{m-1}).  Face j lies between rows j and j+1.  State: for
-// w1/w3 P_{m-2}, t_{m-2}, A_{m-2}; for w2/w4 Q_{m-2}, D_{m-2}, c_{m-2}.
+// The per-column y-pipeline.  Row m arrives x-swept; with row m-1 it gives the face
+// differences D_{m-1}.  left() advances the left-moving invariants, apply() adds the
+// increments of row m-2 to its fields, right() advances the right-moving invariants.
+// Face j lies between rows j and j+1.
 template <typename T, int V>
-struct YPipe {
-  T p2[2][V], t2[2][V], a2[2][V], q2[2][V], d2[2][V], c2[2][V];
-  T dfw[2][V], bo[2][V];
+struct YPipe;
+
+// FP64: the reference's flux form (as sweep_x_lane_exact, along y).  left() forms
+// G_{m-1} = w_{m-1} - psi'_{m-1} D_{m-2} and the left-moving flux difference of row m-2,
+// G_{m-2} - G_{m-1}; apply() completes row m-2 from its invariants and both flux
+// differences; right() forms F_{m-1} = w_{m-1} + psi_{m-1} D_{m-1} and the right-moving
+// flux difference of row m-1, F_{m-1} - F_{m-2}.  State: for w1/w3 P_{m-2}, F_{m-2} and
+// that difference; for w2/w4 Q_{m-2}, D_{m-2}, G_{m-2}.
+template <int V>
+struct YPipe<double, V> {
+  double p2[2][V], f2[2][V], dr[2][V], q2[2][V], d2[2][V], g2[2][V];
+  double dfw[2][V], wr[2][V], dl[2][V];  // this row's D_{m-1} and w_{m-1} of w1/w3; row m-2's left difference
 
   __device__ __forceinline__ void init() {
 #pragma unroll
     for (int v = 0; v < V; ++v)
 #pragma unroll
-      for (int q = 0; q < 2; ++q) p2[q][v] = t2[q][v] = a2[q][v] = q2[q][v] = d2[q][v] = c2[q][v] = T(0);
+      for (int q = 0; q < 2; ++q) p2[q][v] = f2[q][v] = dr[q][v] = q2[q][v] = d2[q][v] = g2[q][v] = 0.0;
   }
 
-  __device__ __forceinline__ void left(const T (&f)[NF][V], const T (&pvy)[V], const T (&psyy)[V],
-                                       const T (&pvx)[V], const T (&psxy)[V], const Sweep<T>& cy) {
-    const T eps = tvd_eps<T>();
+  __device__ __forceinline__ void left(const double (&f)[NF][V], const double (&pvy)[V],
+                                       const double (&psyy)[V], const double (&pvx)[V],
+                                       const double (&psxy)[V], const Sweep<double>& cy) {
+    const double eps = tvd_eps<double>();
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-      T d[4];
-      face_differences(f[VY][v] - pvy[v], f[SYY][v] - psyy[v], f[VX][v] - pvx[v],
-                       f[SXY][v] - psxy[v], cy, d[0], d[1], d[2], d[3]);
+      double wc[4], wp[4];  // invariants of rows m and m-1 (omega_y: vn = vy, sn = syy, vt = vx)
+      ex::invariants(f[VY][v], f[SYY][v], f[VX][v], f[SXY][v], cy, wc);
+      ex::invariants(pvy[v], psyy[v], pvx[v], psxy[v], cy, wp);
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const T kc = q ? cy.kc2 : cy.kc1;
-        dfw[q][v] = d[2 * q];
-        const T dd = d[2 * q + 1];
-        const T q1 = eps - dd;
-        const T ps = psi(ratio(q1, q2[q][v]), kc);
-        bo[q][v] = fma(-ps, d2[q][v], c2[q][v]);
-        c2[q][v] = fma(ps, d2[q][v], dd);
+        const double kc = q ? cy.kc2 : cy.kc1;
+        dfw[q][v] = ex::sub(wc[2 * q], wp[2 * q]);
+        wr[q][v] = wp[2 * q];
+        const double dd = ex::sub(wc[2 * q + 1], wp[2 * q + 1]);
+        const double q1 = ex::sub(eps, dd);
+        const double ps = psi(ratio(q1, q2[q][v]), kc);
+        const double g1 = ex::sub(wp[2 * q + 1], ex::mul(ps, d2[q][v]));
+        dl[q][v] = ex::sub(g2[q][v], g1);
+        g2[q][v] = g1;
         d2[q][v] = dd;
         q2[q][v] = q1;
       }
     }
   }
 
-  __device__ __forceinline__ void apply(T (&gf)[NF][V], const Sweep<T>& cy) const {
+  __device__ __forceinline__ void apply(double (&gf)[NF][V], const Sweep<double>& cy) const {
 #pragma unroll
-    for (int v = 0; v < V; ++v)
-      apply_increment<1>(gf[VX][v], gf[VY][v], gf[SXX][v], gf[SXY][v], gf[SYY][v], a2[0][v],
-                         bo[0][v], a2[1][v], bo[1][v], cy);
+    for (int v = 0; v < V; ++v) {
+      double w[4];
+      ex::invariants(gf[VY][v], gf[SYY][v], gf[VX][v], gf[SXY][v], cy, w);
+      const double c1 = ex::change(w[0], cy.k1, dr[0][v]);
+      const double c2 = ex::change(w[1], cy.k1, dl[0][v]);
+      const double c3 = ex::change(w[2], cy.k2, dr[1][v]);
+      const double c4 = ex::change(w[3], cy.k2, dl[1][v]);
+      ex::increment<1>(gf[VX][v], gf[VY][v], gf[SXX][v], gf[SXY][v], gf[SYY][v], c1, c2, c3, c4, cy);
+    }
   }
 
-  __device__ __forceinline__ void right(const Sweep<T>& cy) {
-    const T eps = tvd_eps<T>();
+  __device__ __forceinline__ void right(const Sweep<double>& cy) {
+    const double eps = tvd_eps<double>();
 #pragma unroll
     for (int v = 0; v < V; ++v) {
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const T kc = q ? cy.kc2 : cy.kc1;
-        const T dd = dfw[q][v];
-        const T p1 = dd + eps;
-        const T ps = psi(ratio(p2[q][v], p1), kc);
-        a2[q][v] = fma(-ps, dd, t2[q][v]);
-        t2[q][v] = fma(ps, dd, -dd);
+        const double kc = q ? cy.kc2 : cy.kc1;
+        const double dd = dfw[q][v];
+        const double p1 = ex::add(dd, eps);
+        const double ps = psi(ratio(p2[q][v], p1), kc);
+        const double f1 = ex::add(wr[q][v], ex::mul(ps, dd));
+        dr[q][v] = ex::sub(f1, f2[q][v]);
+        f2[q][v] = f1;
         p2[q][v] = p1;
       }
     }

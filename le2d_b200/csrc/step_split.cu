@@ -34,6 +34,27 @@ __device__ __forceinline__ T tvd2(T c, T u_2, T u_1, T u, T u1) {
   return u - c * (f12 - f_12);
 }
 
+// FP64: le_min / le_max / le_max3 (simple/le_core.c:31-33) as written, so NaN and signed
+// zeros come out as in the reference.
+__device__ __forceinline__ double ref_min(double a, double b) { return a > b ? b : a; }
+__device__ __forceinline__ double ref_max(double a, double b) { return a > b ? a : b; }
+
+// FP64 tvd2 operation by operation in uncontracted arithmetic, with IEEE division: the
+// reference double build's result bit for bit.
+template <>
+__device__ __forceinline__ double tvd2<double>(double c, double u_2, double u_1, double u, double u1) {
+  using namespace ex;
+  const double eps = tvd_eps<double>();
+  const double r = add(sub(u, u_1), eps) / add(sub(u1, u), eps);
+  const double r_1 = add(sub(u_1, u_2), eps) / add(sub(u, u_1), eps);
+  const double hc = mul(0.5, sub(1.0, c));  // (1 - c) / 2: halving is exact
+  const double s = ref_max(0.0, ref_max(ref_min(1.0, r + r), ref_min(2.0, r)));
+  const double s_1 = ref_max(0.0, ref_max(ref_min(1.0, r_1 + r_1), ref_min(2.0, r_1)));
+  const double f12 = add(u, mul(mul(s, hc), sub(u1, u)));
+  const double f_12 = add(u_1, mul(mul(s_1, hc), sub(u, u_1)));
+  return sub(u, mul(c, sub(f12, f_12)));
+}
+
 // Index of stencil node q along a line of n nodes: clamped, or (far_rot, y only) the
 // rows n-5, n-4 past the end as le_step_soa sees them.
 __device__ __forceinline__ int line_index(int q, int n, int far_rot) {
@@ -62,26 +83,38 @@ __global__ void sweep_plain_kernel(const T* __restrict__ src, T* __restrict__ ds
     T fv[NF];
 #pragma unroll
     for (int k = 0; k < NF; ++k) fv[k] = b[k * plane];
-    omega<AXIS>(fv[VX], fv[VY], fv[SXX], fv[SXY], fv[SYY], c, w[o + 2][0], w[o + 2][1],
-                w[o + 2][2], w[o + 2][3]);
+    if constexpr (sizeof(T) == 8) {
+      const T vn = AXIS == 0 ? fv[VX] : fv[VY], vt = AXIS == 0 ? fv[VY] : fv[VX];
+      const T sn = AXIS == 0 ? fv[SXX] : fv[SYY];
+      ex::invariants(vn, sn, vt, fv[SXY], c, w[o + 2]);
+    } else {
+      omega<AXIS>(fv[VX], fv[VY], fv[SXX], fv[SXY], fv[SYY], c, w[o + 2][0], w[o + 2][1],
+                  w[o + 2][2], w[o + 2][3]);
+    }
     if (o == 0)
 #pragma unroll
       for (int k = 0; k < NF; ++k) node[k] = fv[k];
   }
-  // reconstruct (simple/le_core.c:251-257), halved as in inc_x / inc_y
-  const T d1 = T(0.5) * (tvd2(k1, w[0][0], w[1][0], w[2][0], w[3][0]) - w[2][0]);
-  const T d2 = T(0.5) * (tvd2(k1, w[4][1], w[3][1], w[2][1], w[1][1]) - w[2][1]);
-  const T d3 = T(0.5) * (tvd2(k2, w[0][2], w[1][2], w[2][2], w[3][2]) - w[2][2]);
-  const T d4 = T(0.5) * (tvd2(k2, w[4][3], w[3][3], w[2][3], w[1][3]) - w[2][3]);
-  T& vn = AXIS == 0 ? node[VX] : node[VY];
-  T& vt = AXIS == 0 ? node[VY] : node[VX];
-  T& sn = AXIS == 0 ? node[SXX] : node[SYY];
-  T& so = AXIS == 0 ? node[SYY] : node[SXX];
-  vn += d1 + d2;
-  vt += d3 + d4;
-  sn += (d2 - d1) * c.rhoc1;
-  so += (d2 - d1) * c.rhoc3;
-  node[SXY] += c.rhoc2 * (d4 - d3);
+  // reconstruct (simple/le_core.c:251-257): the change of each invariant
+  const T c1 = tvd2(k1, w[0][0], w[1][0], w[2][0], w[3][0]) - w[2][0];
+  const T c2 = tvd2(k1, w[4][1], w[3][1], w[2][1], w[1][1]) - w[2][1];
+  const T c3 = tvd2(k2, w[0][2], w[1][2], w[2][2], w[3][2]) - w[2][2];
+  const T c4 = tvd2(k2, w[4][3], w[3][3], w[2][3], w[1][3]) - w[2][3];
+  if constexpr (sizeof(T) == 8) {
+    ex::increment<AXIS>(node[VX], node[VY], node[SXX], node[SXY], node[SYY], c1, c2, c3, c4, c);
+  } else {
+    // inc_x / inc_y (simple/le_core.c:221-249)
+    const T d1 = T(0.5) * c1, d2 = T(0.5) * c2, d3 = T(0.5) * c3, d4 = T(0.5) * c4;
+    T& vn = AXIS == 0 ? node[VX] : node[VY];
+    T& vt = AXIS == 0 ? node[VY] : node[VX];
+    T& sn = AXIS == 0 ? node[SXX] : node[SYY];
+    T& so = AXIS == 0 ? node[SYY] : node[SXX];
+    vn += d1 + d2;
+    vt += d3 + d4;
+    sn += (d2 - d1) * c.rhoc1;
+    so += (d2 - d1) * c.rhoc3;
+    node[SXY] += c.rhoc2 * (d4 - d3);
+  }
   T* o = dst + (long long)j * pitch + i;
 #pragma unroll
   for (int k = 0; k < NF; ++k) o[k * plane] = node[k];
