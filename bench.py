@@ -18,9 +18,16 @@ Our arm (default) prints one JSON line with
             a launch of temporal-block depth 2 advances every node two steps, so its
             algorithmic bytes are 2 x 40 B per node while it moves about half of that,
   cpu_baseline  the reference's own simple/ solver (oracle/_ref) on the host cores,
-  fp64      the same measurement for the FP64 library (80 B per node-update).
+  fp64      the same measurement for the FP64 library (80 B per node-update),
+  batched   256 uneven FP32 solves (sides 128-2048, steps 200-2000) in the persistent
+            batched kernel against the plain one-instance-at-a-time le_step loop on the
+            same GPU: solves/s of both, the speed-up, and the FP32 fields of every instance
+            against the FP64 library's (which equals the reference double build),
+  serving   Poisson request streams (10 and 200 requests/s) through the serving loop:
+            solves/s and p50/p99 latency beside a one-at-a-time plain le_step server.
 Under torchrun each rank solves its own instance (independent solves, weak scaling);
-value is the total node-updates of all ranks over the slowest rank's time.
+value is the total node-updates of all ranks over the slowest rank's time; the batched
+and serving measurements run only in the one-process case.
 
 --impl reference: the reference's own CPU solver (simple/ le_step, OpenMP over all
 host threads) on a bounded sample of the same workload (one time step per bench
@@ -354,29 +361,32 @@ def solve_plain(lib, p, per_call=True, stype=capi.ST_AOS, timing=None):
         lib.le_free_task(t)
 
 
-def run_batched(args):
-    """256 uneven FP32 solves in the persistent batched kernel vs the plain one-at-a-time loop."""
-    from oracle.oracle import fields, rel_l2
+def batched_measure(args, accuracy="all"):
+    """256 uneven FP32 solves in the persistent batched kernel (autotuned, graph-captured
+    windows) against the plain one-instance-at-a-time le_step loop on the same mix.
+
+    accuracy="all": every instance's FP32 fields against the FP64 library's (the same mix
+    through the FP64 batched path; the FP64 library equals the reference double build value
+    for value), per field and relative to the whole state's norm, plus the reference's own
+    float-vs-double error on the worst instance (the C oracle reproduces both builds bit for
+    bit).  accuracy="smallest4" (the standalone mode): also the 4 smallest instances against
+    the reference float and double builds."""
+    from oracle.oracle import Oracle, fields, rel_l2
 
     probs = workloads.batched_256()
     lib = capi.Lib("f")
-    libd = capi.Lib("d")
     nu = sum(p.node_updates for p in probs)
-    budget = int(1.1 * sum(2 * 5 * 4 * (((p.nx + 31) // 32) * 32) * p.ny for p in probs)) + (64 << 20)
 
-    def batch_run(scale_steps=None):
-        with capi.Batch(lib, budget) as b:
-            ids = []
-            for p in probs:
-                q = p if scale_steps is None else workloads.Problem(**{**p.__dict__, "steps": scale_steps})
-                ids.append(b.add(b.problem(q), disks=q.disks))
-            assert all(i >= 0 for i in ids)
-            t0 = time.perf_counter()
-            rc, ms = b.run(window_steps=args.window)
-            wall = time.perf_counter() - t0
-            assert rc == 0, lib.strerror(rc)
-            outs = [b.fields(i) for i in ids] if scale_steps is None else None
-            return ms, wall, outs
+    def budget_of(itemsize):
+        return int(1.1 * sum(2 * 5 * itemsize * (((p.nx + 31) // 32) * 32) * p.ny + 512 for p in probs)) + (64 << 20)
+
+    def add_all(b, scale_steps=None):
+        ids = []
+        for p in probs:
+            q = p if scale_steps is None else workloads.Problem(**{**p.__dict__, "steps": scale_steps})
+            ids.append(b.add(b.problem(q), disks=q.disks))
+        assert all(i >= 0 for i in ids)
+        return ids
 
     # batched-path autotuner: tile height and steps per work item for every size class of the
     # mix (outside the timed region; the table then applies to the instances added below)
@@ -390,70 +400,118 @@ def run_batched(args):
                 plan, nus = lib.batch_autotune(p.nx, p.ny)
                 tuned[key] = {**plan, "nu_s": nus}
         tune_s = time.perf_counter() - t0
-    batch_run(scale_steps=8)  # warm-up (kernels, allocations)
-    ms, wall, outs = batch_run()
-    # the plain loop: every instance alone, one le_step call per step
-    loop_only = [0.0]
-    t0 = time.perf_counter()
-    for p in probs:
-        solve_plain(lib, p, per_call=True, timing=loop_only)
-    plain_s = time.perf_counter() - t0
-    loop_only_n = [0.0]
-    t0 = time.perf_counter()
-    for p in probs:
-        solve_plain(lib, p, per_call=False, timing=loop_only_n)
-    plain_n_s = time.perf_counter() - t0
-    # accuracy of the 4 smallest instances (most steps per node, most reflections): our FP32
-    # against the FP64 library (itself checked against the reference), beside the reference's
-    # own float build against its double build on the same problem (the C oracle reproduces
-    # both bit for bit), and the error relative to the norm of the whole state
-    from oracle.oracle import Oracle
+    with capi.Batch(lib, budget_of(4)) as b:  # warm-up (kernels, allocations)
+        add_all(b, scale_steps=8)
+        assert b.run(window_steps=args.window)[0] == 0
+    bf = capi.Batch(lib, budget_of(4))
+    try:
+        ids = add_all(bf)
+        t0 = time.perf_counter()
+        rc, ms = bf.run(window_steps=args.window)
+        wall = time.perf_counter() - t0
+        assert rc == 0, lib.strerror(rc)
+        # the plain loop: every instance alone, one le_step call per step
+        loop_only = [0.0]
+        t0 = time.perf_counter()
+        for p in probs:
+            solve_plain(lib, p, per_call=True, timing=loop_only)
+        plain_s = time.perf_counter() - t0
+        out = {
+            "metric": "solves/s", "value": len(probs) / (ms * 1e-3), "unit": "solves/s",
+            "workload": "batched_256: 256 FP32 solves, sides log-uniform 128-2048, c1 U[1,4], c2/c1 U[0.3,0.6], "
+                        "rho U[1,3], dt=0.5h/c1, 1-4 disks, steps U[200,2000]",
+            "node_updates": nu, "batched_device_s": ms * 1e-3, "batched_wall_s": wall,
+            "batched_nu_s": nu / (ms * 1e-3), "window_steps": args.window,
+            "autotune": {"seconds": tune_s, "classes": {f"2^{a}x2^{b}": v for (a, b), v in sorted(tuned.items())}},
+            "plain_le_step_loop_s": plain_s, "plain_le_step_solves_s": len(probs) / plain_s,
+            "plain_le_step_loop_steps_only_s": loop_only[0],
+            "speedup_vs_plain_le_step": plain_s / (ms * 1e-3),
+            "speedup_vs_plain_le_step_steps_only": loop_only[0] / (ms * 1e-3),
+            "plain": "each instance alone through le_init_task, le_set_ball, one le_step call per step, "
+                     "download of the final fields (the reference's driver loop on the GPU library)",
+        }
+        if accuracy == "smallest4":
+            loop_only_n = [0.0]
+            t0 = time.perf_counter()
+            for p in probs:
+                solve_plain(lib, p, per_call=False, timing=loop_only_n)
+            plain_n_s = time.perf_counter() - t0
+            out.update({"plain_step_n_loop_s": plain_n_s, "plain_step_n_solves_s": len(probs) / plain_n_s,
+                        "plain_step_n_loop_steps_only_s": loop_only_n[0],
+                        "speedup_vs_plain_step_n": plain_n_s / (ms * 1e-3)})
+        # accuracy over the whole mix: FP32 against the FP64 library, instance by instance
+        libd = capi.Lib("d")
+        with capi.Batch(libd, budget_of(8)) as bd:
+            idd = add_all(bd)
+            rcd, msd = bd.run(window_steps=args.window)
+            assert rcd == 0, libd.strerror(rcd)
+            per_field, state_rel, worst_k = [], [], 0
+            for k, p in enumerate(probs):
+                ours = fields(bf.fields(ids[k]), p.nx, p.ny, 1)
+                ref = fields(bd.fields(idd[k]), p.nx, p.ny, 1)
+                e = rel_l2(ours, ref)
+                per_field.append(e)
+                d = ours.astype(np.float64) - ref
+                state_rel.append(float(np.sqrt((d * d).sum() / (ref * ref).sum())))
+                if e.max() > per_field[worst_k].max():
+                    worst_k = k
+        per_field = np.array(per_field)
+        wp = probs[worst_k]
+        acc = {"instances": len(probs), "fp64_batched_device_s": msd * 1e-3,
+               "max_rel_l2_per_field": per_field.max(axis=0).tolist(),
+               "median_rel_l2_per_field": np.median(per_field, axis=0).tolist(),
+               "instances_over_1e-5_any_field": int((per_field.max(axis=1) > 1e-5).sum()),
+               "max_state_rel_l2": max(state_rel), "median_state_rel_l2": float(np.median(state_rel)),
+               "worst_instance": {"index": worst_k, "nx": wp.nx, "ny": wp.ny, "steps": wp.steps,
+                                  "ours_fp32_vs_fp64_rel_l2": per_field[worst_k].tolist(),
+                                  "ours_fp32_vs_fp64_state_rel_l2": state_rel[worst_k]}}
+        if wp.node_updates <= 6e7:  # the reference's own float build on the worst instance
+            refs = {}
+            for prec in ("f", "d"):
+                o = Oracle(prec)
+                g = np.zeros(5 * wp.nx * wp.ny, o.dtype)
+                for dd in wp.disks:
+                    o.set_ball(g, wp.nx, wp.ny, wp.hx, wp.hy, 1, *dd)
+                o.run(g, wp.nx, wp.ny, wp.dt, wp.hx, wp.hy, wp.c1, wp.c2, wp.rho, 1, wp.steps)
+                refs[prec] = fields(g, wp.nx, wp.ny, 1)
+            acc["worst_instance"]["reference_float_vs_double_rel_l2"] = rel_l2(refs["f"], refs["d"]).tolist()
+        out["accuracy_fp32_vs_fp64"] = acc
+        if accuracy == "smallest4":
+            rows = []
+            for k in sorted(range(len(probs)), key=lambda k: probs[k].node_updates)[:4]:
+                p = probs[k]
+                ours = fields(bf.fields(ids[k]), p.nx, p.ny, 1)
+                refs = {}
+                for prec in ("f", "d"):
+                    o = Oracle(prec)
+                    g = np.zeros(5 * p.nx * p.ny, o.dtype)
+                    for dd in p.disks:
+                        o.set_ball(g, p.nx, p.ny, p.hx, p.hy, 1, *dd)
+                    o.run(g, p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, 1, p.steps)
+                    refs[prec] = fields(g, p.nx, p.ny, 1)
+                rows.append({"instance": k, "nx": p.nx, "ny": p.ny, "steps": p.steps,
+                             "ours_fp32_vs_reference_double_rel_l2": rel_l2(ours, refs["d"]).tolist(),
+                             "ours_fp32_vs_reference_float_rel_l2": rel_l2(ours, refs["f"]).tolist(),
+                             "reference_float_vs_double_rel_l2": rel_l2(refs["f"], refs["d"]).tolist()})
+            out["accuracy_4_smallest"] = rows
+    finally:
+        bf.close()
+    return out
 
-    acc = []
-    for k in sorted(range(len(probs)), key=lambda k: probs[k].node_updates)[:4]:
-        p = probs[k]
-        ref = fields(solve_plain(libd, p, per_call=False), p.nx, p.ny, 1)
-        ours = fields(outs[k], p.nx, p.ny, 1)
-        refs = {}
-        for prec in ("f", "d"):
-            o = Oracle(prec)
-            g = np.zeros(5 * p.nx * p.ny, o.dtype)
-            for d in p.disks:
-                o.set_ball(g, p.nx, p.ny, p.hx, p.hy, 1, *d)
-            o.run(g, p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, 1, p.steps)
-            refs[prec] = fields(g, p.nx, p.ny, 1)
-        state_rel = float(np.sqrt(((ours.astype(np.float64) - ref) ** 2).sum() / (ref**2).sum()))
-        acc.append({"instance": k, "nx": p.nx, "ny": p.ny, "steps": p.steps,
-                    "ours_fp32_vs_fp64_rel_l2": rel_l2(ours, ref).tolist(),
-                    "reference_float_vs_double_rel_l2": rel_l2(refs["f"], refs["d"]).tolist(),
-                    "ours_fp32_vs_fp64_state_rel_l2": state_rel})
-    worst = np.max([a["ours_fp32_vs_fp64_rel_l2"] for a in acc], axis=0)
-    line = {
-        "metric": "solves/s", "value": len(probs) / (ms * 1e-3), "unit": "solves/s", "n_gpus": 1,
-        "workload": "batched_256: 256 FP32 solves, sides log-uniform 128-2048, c1 U[1,4], c2/c1 U[0.3,0.6], "
-                    "rho U[1,3], dt=0.5h/c1, 1-4 disks, steps U[200,2000]",
-        "node_updates": nu, "batched_device_s": ms * 1e-3, "batched_wall_s": wall,
-        "batched_nu_s": nu / (ms * 1e-3), "window_steps": args.window,
-        "autotune": {"seconds": tune_s, "classes": {f"2^{a}x2^{b}": v for (a, b), v in sorted(tuned.items())}},
-        "plain_le_step_loop_s": plain_s, "plain_le_step_solves_s": len(probs) / plain_s,
-        "plain_le_step_loop_steps_only_s": loop_only[0],
-        "plain_step_n_loop_s": plain_n_s, "plain_step_n_solves_s": len(probs) / plain_n_s,
-        "plain_step_n_loop_steps_only_s": loop_only_n[0],
-        "speedup_vs_plain_le_step": plain_s / (ms * 1e-3), "speedup_vs_plain_step_n": plain_n_s / (ms * 1e-3),
-        "speedup_vs_plain_le_step_steps_only": loop_only[0] / (ms * 1e-3),
-        "max_rel_l2_vs_fp64_4_smallest": worst.tolist(),
-        "accuracy_4_smallest": acc,
-    }
+
+def run_batched(args):
+    """256 uneven FP32 solves in the persistent batched kernel vs the plain one-at-a-time loop."""
+    line = batched_measure(args, accuracy="smallest4")
+    line["n_gpus"] = 1
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_serving(args):
+def serving_measure(args, rates):
     """Poisson request streams through the serving loop vs a one-at-a-time plain le_step server."""
     import threading
 
     lib = capi.Lib("f")
-    rates = [float(r) for r in args.rates.split(",")]
     out = {"metric": "serving", "workload": "serving_stream: Poisson arrivals, sides log-uniform 64-4096, "
                                             "materials/disks as the batched workload, steps U[100,5000], "
                                             "half fields / half receiver lines (vx,vy at row ny/4 every 10 steps)",
@@ -479,17 +537,19 @@ def run_serving(args):
             th = threading.Thread(target=submitter)
             th.start()
             th.join()
-            lat, first, last = [], None, 0.0
+            lat, spans = [], []
             for k, t in enumerate(tickets):
                 assert t > 0 and srv.wait(t, 600.0) == 0
-                a, _, c = srv.times(t)
-                lat.append(c - a)
-                first = a if first is None else min(first, a)
-                last = max(last, c)
+                s_, a, c = srv.times(t)
+                lat.append(c - s_)
+                spans.append((a, c))
                 srv.release(t)
             st = srv.stats()
+        first = min(a for a, _ in spans)
+        last = max(c for _, c in spans)
+        joined = sum(1 for b in spans if any(a[0] < b[0] < a[1] for a in spans if a is not b))
         # one-at-a-time plain le_step server on the same stream (FIFO, no overlap)
-        plat, t0, busy_until = [], time.perf_counter(), 0.0
+        plat, t0 = [], time.perf_counter()
         for r in reqs:
             now = time.perf_counter() - t0
             if now < r.arrival_s:
@@ -502,9 +562,15 @@ def run_serving(args):
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "plain_solves_s": len(reqs) / plain_total, "plain_p50_s": float(np.percentile(plat, 50)),
             "plain_p99_s": float(np.percentile(plat, 99)), "windows": st["windows"],
+            "admitted_while_others_ran": joined,
         })
         print(json.dumps(out["rates"][-1]), file=sys.stderr, flush=True)
-    print(json.dumps(out), flush=True)
+    out["latency"] = "submission to completion (s); plain: arrival to completion"
+    return out
+
+
+def run_serving(args):
+    print(json.dumps(serving_measure(args, [float(r) for r in args.rates.split(",")])), flush=True)
     return 0
 
 
@@ -667,6 +733,9 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 leg")
     ap.add_argument("--no-tune", action="store_true", help="batched: skip the batched-path autotuner")
     ap.add_argument("--time-steps", type=int, default=None, help="time steps per solve (default 1000)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="single: skip the batched and serving measurements added to the line")
+    ap.add_argument("--extra-rates", default="10,200", help="single: serving request rates in the line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -741,6 +810,10 @@ def main():
                                      "kernel": (f"{'fused_pair_kernel' if d_plan['warps_per_task'] == 2 else 'fused_step_kernel'}"
                                                 f"<double, V={d_plan['lanes']}, depth={d_depth}>")},
                         "clocks": d_clk}
+    if world == 1 and not args.no_extras:
+        # the batched and serving targets on the same GPU (one process; skipped under torchrun)
+        line["batched"] = batched_measure(args)
+        line["serving"] = serving_measure(args, [float(r) for r in args.extra_rates.split(",")])
     if rank == 0 and not args.no_cpu:
         cb = cpu_reference_sample(p)
         line["cpu_baseline"] = cb["simple"]

@@ -112,8 +112,9 @@ int le2d_diagnostics(le_task *task, le2d_diag_t *out);
  * repeated calls give identical results) for at most LE2D_DIAG_NOALLOC_MAX_ROWS rows
  * (larger grids: LE2D_EINVAL); every GPU that loads the library holds it (~1.4 MB)
  * until exit.  All calls share it: calls whose kernels overlap on the GPU race.  The
- * first call on a device looks up the array's device address; make that first call
- * before any stream capture. */
+ * first call on a device (and the first after a reset of that device) looks up the
+ * array's device address; make that first call before any stream capture.  Each call
+ * synchronises `stream` before it returns (it reads the result back to *out). */
 #define LE2D_DIAG_NOALLOC_MAX_ROWS 16384
 int le2d_diagnostics_noalloc(const real *d_state, int nx, int ny, long long pitch,
 			     long long plane, real hx, real hy, real c1, real c2, real rho,
@@ -146,7 +147,10 @@ void le2d_batch_destroy(le2d_batch *b);
  * or -LE2D_E* (e.g. -LE2D_EBUDGET when it does not fit the budget). */
 int le2d_batch_add(le2d_batch *b, const le2d_problem *p, const real *init, int ndisks,
 		   const real *disks);
-/* Runs every instance to its step count; *device_ms (may be NULL) = device time. */
+/* Runs every instance to its step count; *device_ms (may be NULL) = device time.
+ * LE2D_ETIMEOUT if a bounded wait gave up: only the instances concerned fail (their
+ * le2d_batch_fields / _receivers / _diagnostics return LE2D_ETIMEOUT), the others'
+ * results are valid. */
 int le2d_batch_run(le2d_batch *b, int window_steps, float *device_ms);
 int le2d_batch_count(const le2d_batch *b);
 /* Final fields of instance `id` (5*nx*ny reals, the problem's layout). */
@@ -155,8 +159,8 @@ int le2d_batch_fields(le2d_batch *b, int id, real *out);
  * sample s (after step (s+1)*receiver_every); *nsamples = steps / receiver_every. */
 int le2d_batch_receivers(le2d_batch *b, int id, real *out, int *nsamples);
 int le2d_batch_diagnostics(le2d_batch *b, int id, le2d_diag_t *out);
-/* Bounded dependency waits: the kernel gives up after this many ns (default 2e9) and
- * le2d_batch_run returns LE2D_ETIMEOUT. */
+/* Bounded dependency waits: the kernel gives up on an instance after this many ns
+ * (default 2e9), skips its remaining work and le2d_batch_run returns LE2D_ETIMEOUT. */
 int le2d_batch_set_wait_limit(le2d_batch *b, unsigned long long ns);
 /* Batched-path autotuner: times the batched kernel on copies of a scratch problem of
  * nx x ny nodes (enough copies for ~24 M nodes) for every tile height (16 ... 256 rows) and
@@ -171,10 +175,13 @@ int le2d_batch_autotune_reset(void);
 
 /* ---- Served solves (continuous batching) --------------------------------------------
  * A background loop owns a device arena of `device_budget_bytes`.  Requests are queued
- * by le2d_server_submit (thread-safe, returns at once); between windows of
- * `window_steps` steps the loop admits queued requests while their states fit the
- * budget (and at most `max_active` run at once), advances every admitted solve in one
- * persistent launch, and moves finished ones to host-side results. */
+ * by le2d_server_submit (thread-safe, returns at once); the loop admits queued requests
+ * while their states fit the budget (and at most `max_active` run at once), advances
+ * every admitted solve in persistent launches of `window_steps` steps, and moves
+ * finished ones to host-side results.  Initial states are uploaded and results read
+ * back on a copy stream while the next launch runs; requests that arrive during a
+ * launch join the next one.  A solve whose bounded device wait gives up fails alone
+ * (LE2D_ETIMEOUT). */
 #define LE2D_WANT_FIELDS 0
 #define LE2D_WANT_RECEIVERS 1
 

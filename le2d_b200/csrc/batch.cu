@@ -14,10 +14,14 @@
 // done[n] >= r for every neighbour n (and t itself); after the tile it publishes
 // done[t] = r + 1 with release semantics.  Items are claimed in order and a claimed
 // item only waits on items of smaller index, all held by running warps, so the
-// smallest unfinished item can always proceed.  Every wait is bounded: after
-// `wait_ns` of global time (or once another warp has given up) the warp sets
-// ctl->status and leaves; the host reads the status (LE2D_ETIMEOUT), the context stays
-// usable.  State loads use ld.global.cg: other warps of this launch write them.
+// smallest unfinished item can always proceed.  Every wait is bounded.  A dependency
+// wait that runs out (after `wait_ns` of global time) marks its instance failed (the
+// instance's failure word) and the warp moves on; every later item of that instance --
+// the only items that depend on the missing tile -- is skipped, so the other instances
+// of the launch finish normally.  A wait between the two warps of a pair that runs out
+// sets ctl->status and ends the launch.  The host reads both (LE2D_ETIMEOUT for the
+// failed instances, or for all), the context stays usable.  State loads use
+// ld.global.cg: other warps of this launch write them.
 //
 // FP32 items advance two steps (temporal blocking) on a producer / consumer warp pair
 // (march_pair.cuh): the producer claims the item, passes its index to the consumer through
@@ -53,10 +57,21 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+// True (warp-uniformly) if the instance has failed or the launch is ending.
+__device__ __forceinline__ bool instance_off(const int* fail, const BatchCtl* ctl) {
+  int off = 0;
+  if ((threadIdx.x & 31) == 0)
+    off = *reinterpret_cast<const volatile int*>(fail) != 0 ||
+          *reinterpret_cast<const volatile int*>(&ctl->status) != 0;
+  return __shfl_sync(0xffffffffu, off, 0) != 0;
+}
+
 // Waits until every tile of the 3x3 neighbourhood of (seg, strip) has done[] >= r.
-// Lanes 0..8 each watch one neighbour.  Returns false if the wait gave up.
+// Lanes 0..8 each watch one neighbour.  Returns false if the item is to be skipped: the
+// wait gave up (the instance is marked failed), the instance failed meanwhile, or the
+// launch is ending (ctl->status).
 __device__ __forceinline__ bool wait_neighbours(const int* done, int tile_base, int nstrips,
-                                                int nsegs, int seg, int strip, int r,
+                                                int nsegs, int seg, int strip, int r, int* fail,
                                                 BatchCtl* ctl, unsigned long long wait_ns) {
   const int lane = threadIdx.x & 31;
   const int ds = lane / 3 - 1, dk = lane % 3 - 1;
@@ -72,9 +87,10 @@ __device__ __forceinline__ bool wait_neighbours(const int* done, int tile_base, 
     if (__all_sync(0xffffffffu, ready)) return true;
     int bail = 0;
     if (lane == 0) {
-      bail = *reinterpret_cast<volatile int*>(&ctl->status) != 0;
+      bail = *reinterpret_cast<volatile int*>(fail) != 0 ||
+             *reinterpret_cast<volatile int*>(&ctl->status) != 0;
       if (!bail && polls >= 1024 && global_ns() - t0 > wait_ns) {
-        atomicExch(&ctl->status, 1);
+        if (atomicExch(fail, 1) == 0) atomicAdd(&ctl->failed, 1);
         bail = 1;
       }
     }
@@ -82,6 +98,20 @@ __device__ __forceinline__ bool wait_neighbours(const int* done, int tile_base, 
     __nanosleep(ns);
     if (ns < 1024) ns *= 2;
   }
+}
+
+// Whether the item of instance I at window step r may run (its dependencies are done).
+template <typename T>
+__device__ __forceinline__ bool item_ready(const BatchInst<T>& I, const BatchTile& bt, int r,
+                                           const int* done, BatchCtl* ctl,
+                                           unsigned long long wait_ns) {
+  if (r == 0) return !instance_off(I.fail, ctl);
+  return wait_neighbours(done, I.tile_base, I.nstrips, I.nsegs, bt.seg, bt.strip, r, I.fail, ctl,
+                         wait_ns);
+}
+
+__device__ __forceinline__ bool launch_ending(const BatchCtl* ctl) {
+  return *reinterpret_cast<const volatile int*>(&ctl->status) != 0;
 }
 
 template <typename T, int V, int MINB>
@@ -102,9 +132,10 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
     while ((long long)q >= step_items[r + 1]) ++r;
     const BatchTile bt = tiles[q - step_items[r]];
     const BatchInst<T>& I = insts[bt.inst];
-    if (r > 0 &&
-        !wait_neighbours(done, I.tile_base, I.nstrips, I.nsegs, bt.seg, bt.strip, r, ctl, wait_ns))
-      break;
+    if (!item_ready(I, bt, r, done, ctl, wait_ns)) {  // the instance failed: skip the item
+      if (launch_ending(ctl)) break;
+      continue;
+    }
     const int par = (I.parity + r) & 1;
     const march::GridRef<T> g{I.buf[par], I.buf[par ^ 1], I.nx, I.ny, I.pitch, I.plane, I.far_rot};
     const int y0 = bt.seg * I.seg_len;
@@ -147,23 +178,29 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
   // The two roles run separate loops (each keeps only its own state live across its march).
   if (producer) {
     while (true) {
-      const int hs = (int)(u % kHand);
       unsigned long long claimed = 0;
       if (lane == 0) claimed = atomicAdd(&ctl->next, 1ULL);
       const long long q = (long long)__shfl_sync(0xffffffffu, claimed, 0);
+      // the item's dependencies first, then the hand-off: a skipped item (its instance
+      // failed) goes to the consumer as -(q + 1)
+      bool skip = false;
+      if (q < total) {
+        while (q >= step_items[r + 1]) ++r;
+        const BatchTile bt = tiles[q - step_items[r]];
+        skip = !item_ready(insts[bt.inst], bt, r, done, ctl, wait_ns);
+        if (skip && launch_ending(ctl)) break;
+      }
+      const int hs = (int)(u % kHand);
       const unsigned use = u / kHand;
       if (use > 0 && !march::mbar_wait(bars + kHand + hs, (use - 1) & 1, wait_ns, status)) break;
-      if (lane == 0) item_q[hs] = q;
+      if (lane == 0) item_q[hs] = skip ? -(q + 1) : q;
       march::mbar_arrive(bars + hs);
       ++u;
       if (q >= total) break;
-      while (q >= step_items[r + 1]) ++r;
+      if (skip) continue;
       const BatchTile bt = tiles[q - step_items[r]];
       const BatchInst<T>& I = insts[bt.inst];
       const int nadv = min(I.depth, I.steps - r * I.depth);  // steps this item advances
-      if (r > 0 &&
-          !wait_neighbours(done, I.tile_base, I.nstrips, I.nsegs, bt.seg, bt.strip, r, ctl, wait_ns))
-        break;
       const int par = (I.parity + r) & 1;
       const march::GridRef<T> g{I.buf[par], I.buf[par ^ 1], I.nx, I.ny, I.pitch, I.plane, I.far_rot};
       const int y0 = bt.seg * I.seg_len;
@@ -179,6 +216,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
       const long long q = item_q[hs];
       march::mbar_arrive(bars + kHand + hs);
       ++u;
+      if (q < 0) continue;  // skipped by the producer: its instance failed
       if (q >= total) break;
       while (q >= step_items[r + 1]) ++r;
       const BatchTile bt = tiles[q - step_items[r]];

@@ -91,10 +91,41 @@ __global__ void __launch_bounds__(kThreads) diag_final_kernel(int ny, double* sc
   block_reduce(acc, scratch + (long long)kNoallocRows * kVals);
 }
 
-// Device address of g_diag_scratch per device, looked up once per device with that device
-// current (a host-side use of the symbol's name is only a stand-in, not a device address).
+// Device address of g_diag_scratch per device, looked up with that device current (a
+// host-side use of the symbol's name is only a stand-in, not a device address): once per
+// device and context -- a reset of the device (cudaDeviceReset) destroys the context whose
+// address was cached, and the next call looks it up again in the new one.
 std::mutex g_mu;
 double* g_addr[64] = {nullptr};
+unsigned long long g_ctx[64] = {0};
+
+// The current context's unique id (driver API cuCtxGetCurrent / cuCtxGetId, reached through
+// the runtime's entry-point query so the library needs no link to the driver library), or 0
+// when unavailable -- then the address is looked up on every call.
+unsigned long long context_id() {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool tried = false;
+  if (!tried) {  // under g_mu
+    tried = true;
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+      get_current = reinterpret_cast<GetCurrent>(f1);
+      get_id = reinterpret_cast<GetId>(f2);
+    }
+    cudaGetLastError();
+  }
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 }  // namespace
 
@@ -121,7 +152,9 @@ extern "C" int le2d_diagnostics_noalloc(const real* d_state, int nx, int ny, lon
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
+    const unsigned long long ctx = context_id();  // 0 before the device's context exists
+    if (!g_addr[dev] || ctx == 0 || ctx != g_ctx[dev]) {
+      g_ctx[dev] = ctx;
       e = cudaGetSymbolAddress((void**)&g_addr[dev], g_diag_scratch);
       if (e != cudaSuccess) {
         g_addr[dev] = nullptr;

@@ -89,20 +89,26 @@ Engine<T>::Engine(size_t budget) {
   if (budget == 0 || budget > avail) budget = (size_t)(0.9 * (double)avail);
   arena_ = new Arena(budget);
   if (cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess) stream_ = nullptr;
+  if (cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking) != cudaSuccess) {
+    if (stream_) cudaStreamDestroy(stream_);
+    stream_ = copy_ = nullptr;
+  }
   cudaEventCreate(&ev_[0]);
   cudaEventCreate(&ev_[1]);
   if (cudaMalloc(&d_diag_, 16 * sizeof(double)) != cudaSuccess) d_diag_ = nullptr;
   int dev = 0;
   cudaGetDevice(&dev);
   resident_blocks_ = batch_resident_blocks<T>(dev);
-  // Test hook for the bounded-wait path: one tile never publishes its first step, so
-  // the launch ends with a timeout status instead of results.
+  // Test hook for the bounded-wait path: in the engine's first window, tile k of the work
+  // list never publishes its first step, so its instance fails (LE2D_ETIMEOUT) while the
+  // other instances finish.
   if (const char* s = getenv("LE2D_TEST_STALL_TILE")) stall_tile_ = atoi(s);
 }
 
 template <typename T>
 Engine<T>::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
+  if (copy_) cudaStreamSynchronize(copy_);
   delete arena_;
   cudaFree(d_insts_);
   cudaFree(d_tiles_);
@@ -113,13 +119,14 @@ Engine<T>::~Engine() {
   if (ev_[0]) cudaEventDestroy(ev_[0]);
   if (ev_[1]) cudaEventDestroy(ev_[1]);
   if (stream_) cudaStreamDestroy(stream_);
+  if (copy_) cudaStreamDestroy(copy_);
 }
 
 template <typename T>
 size_t Engine<T>::footprint(const le2d_problem& p) {
   if (p.nx < 1 || p.ny < 1) return 0;
   const long long pitch = row_pitch_elems(p.nx);
-  size_t b = (sizeof(T) * 2 * 5 * (size_t)pitch * (size_t)p.ny + 255) / 256 * 256;
+  size_t b = (sizeof(T) * 2 * 5 * (size_t)pitch * (size_t)p.ny + 255) / 256 * 256 + 256;  // + failure word
   if (p.receiver_row >= 0 && p.receiver_every > 0)
     b += (sizeof(T) * 2 * (size_t)pitch * (size_t)(p.steps / p.receiver_every) + 255) / 256 * 256;
   return b;
@@ -224,22 +231,22 @@ int batch_autotune(int nx, int ny, BatchTuned* best) {
   return LE2D_OK;
 }
 
+// Validation, arena blocks (both state buffers and the failure word; receiver samples),
+// constants and tiles of a new instance.  Returns LE2D_OK or -LE2D_E*.
 template <typename T>
-int Engine<T>::add(const le2d_problem& p, const T* init, int ndisks, const T* disks) {
+int Engine<T>::alloc_instance(const le2d_problem& p, Inst& in) {
   if (!ok()) return -LE2D_ENODEV;
   if (p.nx < 3 || p.ny < 3 || p.steps < 0 || !(p.hx > 0) || !(p.hy > 0) || !(p.dt > 0) ||
       !(p.c1 > 0) || !(p.c2 > 0) || !(p.rho > 0) || (p.stype != ST_AOS && p.stype != ST_SOA) ||
-      p.receiver_row >= p.ny || (p.receiver_row >= 0 && p.receiver_every < 1) || ndisks < 0 ||
-      (ndisks > 0 && !disks))
+      p.receiver_row >= p.ny || (p.receiver_row >= 0 && p.receiver_every < 1))
     return -LE2D_EINVAL;
   // CFL: the Courant numbers must not exceed 1 (the scheme is stable for k <= 1).
   if ((double)p.dt * p.c1 > (double)std::min(p.hx, p.hy)) return -LE2D_EINVAL;
-  Inst in;
   in.p = p;
   in.pitch = row_pitch_elems(p.nx);
   in.plane = in.pitch * p.ny;
   const size_t sbytes = sizeof(T) * 2 * 5 * (size_t)in.plane;
-  in.state_off = arena_->alloc(sbytes);
+  in.state_off = arena_->alloc(sbytes + 256);
   if (in.state_off == SIZE_MAX) return -LE2D_EBUDGET;
   if (p.receiver_row >= 0) {
     in.nsamples = p.steps / p.receiver_every;
@@ -254,6 +261,7 @@ int Engine<T>::add(const le2d_problem& p, const T* init, int ndisks, const T* di
   }
   in.buf[0] = reinterpret_cast<T*>(arena_->base() + in.state_off);
   in.buf[1] = in.buf[0] + 5 * in.plane;
+  in.fail = reinterpret_cast<int*>(arena_->base() + in.state_off + sbytes);
   in.c = problem_consts<T>(p);
   // Tile height and steps per work item: explicit (autotuner trials), else the autotuner's
   // table for the size class (LE2D_AUTOTUNE=1 tunes a class on first use), else defaults.
@@ -279,7 +287,17 @@ int Engine<T>::add(const le2d_problem& p, const T* init, int ndisks, const T* di
   in.seg_len = std::min(seg, p.ny);
   in.nsegs = (p.ny + in.seg_len - 1) / in.seg_len;
   in.live = true;
-  cudaError_t e = cudaMemsetAsync(in.buf[0], 0, sbytes, stream_);
+  return LE2D_OK;
+}
+
+template <typename T>
+int Engine<T>::add(const le2d_problem& p, const T* init, int ndisks, const T* disks) {
+  if (ndisks < 0 || (ndisks > 0 && !disks)) return -LE2D_EINVAL;
+  Inst in;
+  int rc = alloc_instance(p, in);
+  if (rc) return rc;
+  const size_t sbytes = sizeof(T) * 2 * 5 * (size_t)in.plane;
+  cudaError_t e = cudaMemsetAsync(in.buf[0], 0, sbytes + 256, stream_);  // states, failure word
   if (e == cudaSuccess && in.trace)
     e = cudaMemsetAsync(in.trace, 0, sizeof(T) * 2 * (size_t)in.pitch * in.nsamples, stream_);
   if (e == cudaSuccess && init) {
@@ -304,6 +322,72 @@ int Engine<T>::add(const le2d_problem& p, const T* init, int ndisks, const T* di
 }
 
 template <typename T>
+int Engine<T>::add_async(const le2d_problem& p, const T* init, int ndisks, const T* disks) {
+  if (ndisks < 0 || (ndisks > 0 && !disks)) return -LE2D_EINVAL;
+  Inst in;
+  int rc = alloc_instance(p, in);
+  if (rc) return rc;
+  cudaError_t e = cudaSuccess;
+  if (init) {  // the host state into the second buffer, beside the window in flight
+    e = cudaMemcpyAsync(in.buf[1], init, sizeof(T) * 5 * (size_t)p.nx * p.ny, cudaMemcpyHostToDevice,
+                        copy_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(copy_);  // `init` may be freed on return
+    in.has_init = true;
+  } else {
+    in.disks.assign(disks, disks + 4 * (size_t)ndisks);
+  }
+  if (e != cudaSuccess) {
+    fprintf(stderr, "le2d: batch add: %s\n", cudaGetErrorString(e));
+    arena_->free(in.state_off);
+    if (in.trace) arena_->free(in.trace_off);
+    return -LE2D_ECUDA;
+  }
+  in.prologue = true;
+  insts_.push_back(in);
+  return (int)insts_.size() - 1;
+}
+
+// Initial conditions of instances added by add_async: state and failure word cleared, the
+// uploaded host state packed (or the disks set) -- small kernels queued just before a window.
+template <typename T>
+int Engine<T>::apply_prologues() {
+  cudaError_t e = cudaSuccess;
+  for (Inst& in : insts_) {
+    if (!in.live || !in.prologue) continue;
+    const size_t bytes = sizeof(T) * 5 * (size_t)in.plane;
+    e = cudaMemsetAsync(in.buf[0], 0, bytes, stream_);
+    if (e == cudaSuccess) e = cudaMemsetAsync(in.fail, 0, 256, stream_);
+    if (e == cudaSuccess && in.trace)
+      e = cudaMemsetAsync(in.trace, 0, sizeof(T) * 2 * (size_t)in.pitch * in.nsamples, stream_);
+    if (e == cudaSuccess && in.has_init)
+      e = launch_pack<T>(in.buf[1], in.buf[0], in.p.nx, in.p.ny, in.pitch, in.plane,
+                         in.p.stype == ST_AOS, stream_);
+    for (size_t k = 0; e == cudaSuccess && 4 * k < in.disks.size(); ++k)
+      e = launch_set_ball<T>(in.buf[0], in.p.nx, in.p.ny, in.pitch, in.plane, in.p.hx, in.p.hy,
+                             in.disks[4 * k], in.disks[4 * k + 1], in.disks[4 * k + 2],
+                             in.disks[4 * k + 3], stream_);
+    if (e != cudaSuccess) break;
+    in.prologue = false;
+    in.disks.clear();
+    in.disks.shrink_to_fit();
+  }
+  if (e != cudaSuccess) fprintf(stderr, "le2d: initial condition: %s\n", cudaGetErrorString(e));
+  return e == cudaSuccess ? LE2D_OK : LE2D_ECUDA;
+}
+
+// Reads the failure words of these instances (after a launch that reported failures).
+template <typename T>
+int Engine<T>::read_failures(const std::vector<int>& ids) {
+  for (int id : ids) {
+    Inst& in = insts_[id];
+    int f = 0;
+    if (cudaMemcpy(&f, in.fail, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return LE2D_ECUDA;
+    if (f != 0) in.failed = true;
+  }
+  return LE2D_OK;
+}
+
+template <typename T>
 typename Engine<T>::Window Engine<T>::plan_window(int window, const std::vector<long long>& done,
                                                   const std::vector<int>& cur) const {
   Window w;
@@ -311,7 +395,7 @@ typename Engine<T>::Window Engine<T>::plan_window(int window, const std::vector<
   std::vector<int> steps_of(insts_.size(), 0);
   for (int id = 0; id < (int)insts_.size(); ++id) {
     const Inst& in = insts_[id];
-    if (!in.live) continue;
+    if (!in.live || in.failed) continue;
     const long long left = in.p.steps - done[id];
     if (left <= 0) continue;
     steps_of[id] = (int)std::min<long long>(left, window);
@@ -344,6 +428,7 @@ typename Engine<T>::Window Engine<T>::plan_window(int window, const std::vector<
     b.trace = in.trace;
     b.trace_row = in.trace ? in.p.receiver_row : -1;
     b.trace_every = in.trace ? in.p.receiver_every : 1;
+    b.fail = in.fail;
     w.insts.push_back(b);
     w.inst_ids.push_back(order[k].second);
     w.inst_steps.push_back(steps_of[order[k].second]);
@@ -396,22 +481,27 @@ int Engine<T>::launch_window(const Window& w, size_t io, size_t to, size_t so, s
     e = launch_batch<T>(d_insts_ + io, d_tiles_ + to, d_items_ + so, w.steps, w.step_items.back(),
                         d_done_ + doff, d_ctl_ + co, wait_ns_, stall_tile_ + 1, resident_blocks_,
                         stream_);
+  stall_tile_ = -1;  // the hook stalls one window
   return e == cudaSuccess ? LE2D_OK : LE2D_ECUDA;
 }
 
 template <typename T>
-int Engine<T>::run_window(int window) {
+int Engine<T>::begin_window(int window) {
   if (!ok()) return LE2D_ENODEV;
   if (window < 1) return LE2D_EINVAL;
+  if (in_flight_) return LE2D_ESTATE;
+  int rc = apply_prologues();
+  if (rc) return rc;
   std::vector<long long> done(insts_.size());
   std::vector<int> cur(insts_.size());
   for (size_t i = 0; i < insts_.size(); ++i) {
     done[i] = insts_[i].done_steps;
     cur[i] = insts_[i].cur;
   }
-  Window w = plan_window(window, done, cur);
-  if (w.steps == 0) return LE2D_OK;
-  int rc = ensure_scratch(w.insts.size(), w.tiles.size(), w.step_items.size(), w.tiles.size(), 1);
+  win_ = plan_window(window, done, cur);
+  if (win_.steps == 0) return LE2D_OK;
+  const Window& w = win_;
+  rc = ensure_scratch(w.insts.size(), w.tiles.size(), w.step_items.size(), w.tiles.size(), 1);
   if (rc) return rc;
   cudaError_t e = cudaMemcpyAsync(d_insts_, w.insts.data(), sizeof(BatchInst<T>) * w.insts.size(),
                                   cudaMemcpyHostToDevice, stream_);
@@ -424,13 +514,38 @@ int Engine<T>::run_window(int window) {
   if (e != cudaSuccess) return LE2D_ECUDA;
   rc = launch_window(w, 0, 0, 0, 0, 0);
   if (rc) return rc;
+  // final fields of the instances this window finishes, unpacked into their idle buffer
+  // right after it, so that reading them back needs no kernel beside the next window
+  for (size_t k = 0; k < w.inst_ids.size() && e == cudaSuccess; ++k) {
+    Inst& in = insts_[w.inst_ids[k]];
+    if (in.done_steps + w.inst_steps[k] < in.p.steps) continue;
+    const int c = in.cur ^ (w.inst_items[k] & 1);
+    e = launch_unpack<T>(in.buf[c], in.buf[c ^ 1], in.p.nx, in.p.ny, in.pitch, in.plane,
+                         in.p.stype == ST_AOS, stream_);
+    in.unpacked = true;
+  }
+  if (e != cudaSuccess) return LE2D_ECUDA;
+  in_flight_ = true;
+  return LE2D_OK;
+}
+
+template <typename T>
+int Engine<T>::end_window() {
+  if (!in_flight_) return LE2D_OK;
+  in_flight_ = false;
+  const Window& w = win_;
   BatchCtl ctl;
-  e = cudaMemcpyAsync(&ctl, d_ctl_, sizeof(ctl), cudaMemcpyDeviceToHost, stream_);
+  cudaError_t e = cudaMemcpyAsync(&ctl, d_ctl_, sizeof(ctl), cudaMemcpyDeviceToHost, stream_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
   if (e != cudaSuccess) return LE2D_ECUDA;
-  if (ctl.status != 0) return LE2D_ETIMEOUT;
+  if (ctl.status != 0) {  // a wait inside a warp pair gave up: the launch ended early
+    for (int id : w.inst_ids) insts_[id].failed = true;
+    return LE2D_ETIMEOUT;
+  }
+  if (ctl.failed != 0 && read_failures(w.inst_ids) != LE2D_OK) return LE2D_ECUDA;
   for (size_t k = 0; k < w.inst_ids.size(); ++k) {
     Inst& in = insts_[w.inst_ids[k]];
+    if (in.failed) continue;
     in.done_steps += w.inst_steps[k];
     in.cur ^= w.inst_items[k] & 1;  // each work-item step writes the other buffer
     node_updates_ += (long long)in.p.nx * in.p.ny * w.inst_steps[k];
@@ -439,9 +554,17 @@ int Engine<T>::run_window(int window) {
 }
 
 template <typename T>
+int Engine<T>::run_window(int window) {
+  const int rc = begin_window(window);
+  return rc ? rc : end_window();
+}
+
+template <typename T>
 int Engine<T>::run_all(int window, float* ms) {
   if (!ok()) return LE2D_ENODEV;
   if (window < 1) return LE2D_EINVAL;
+  if (in_flight_) return LE2D_ESTATE;
+  if (apply_prologues() != LE2D_OK) return LE2D_ECUDA;
   std::vector<long long> done(insts_.size());
   std::vector<int> cur(insts_.size());
   for (size_t i = 0; i < insts_.size(); ++i) {
@@ -515,16 +638,34 @@ int Engine<T>::run_all(int window, float* ms) {
   std::vector<BatchCtl> ctl(ws.size());
   e = cudaMemcpy(ctl.data(), d_ctl_, sizeof(BatchCtl) * ws.size(), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return LE2D_ECUDA;
-  for (const BatchCtl& x : ctl)
-    if (x.status != 0) return LE2D_ETIMEOUT;
+  // failures: a launch that ended early fails its instances and every later window's
+  // (their states are not advanced consistently); otherwise only the marked instances
+  bool aborted = false, any_failed = false;
+  for (size_t k = 0; k < ws.size(); ++k) {
+    if (ctl[k].status != 0) aborted = true;
+    if (aborted)
+      for (int id : ws[k].inst_ids) insts_[id].failed = true;
+    if (ctl[k].failed != 0) any_failed = true;
+  }
+  if (any_failed) {
+    std::vector<int> ids;
+    for (int id = 0; id < (int)insts_.size(); ++id)
+      if (insts_[id].live) ids.push_back(id);
+    if (read_failures(ids) != LE2D_OK) return LE2D_ECUDA;
+  }
+  bool failed = false;
   for (const Window& w : ws)
     for (size_t k = 0; k < w.inst_ids.size(); ++k) {
       Inst& in = insts_[w.inst_ids[k]];
+      if (in.failed) {
+        failed = true;
+        continue;
+      }
       in.done_steps += w.inst_steps[k];
       in.cur ^= w.inst_items[k] & 1;
       node_updates_ += (long long)in.p.nx * in.p.ny * w.inst_steps[k];
     }
-  return LE2D_OK;
+  return failed ? LE2D_ETIMEOUT : LE2D_OK;
 }
 
 template <typename T>
@@ -533,10 +674,42 @@ bool Engine<T>::finished(int id) const {
 }
 
 template <typename T>
+bool Engine<T>::failed(int id) const {
+  return id >= 0 && id < (int)insts_.size() && insts_[id].failed;
+}
+
+template <typename T>
+int Engine<T>::harvest_fields(int id, T* out) {
+  if (id < 0 || id >= (int)insts_.size() || !out) return LE2D_EINVAL;
+  const Inst& in = insts_[id];
+  if (!in.live || in.failed || !finished(id)) return in.failed ? LE2D_ETIMEOUT : LE2D_ESTATE;
+  if (!in.unpacked) return fields(id, out);  // no window ran (zero steps)
+  cudaError_t e = cudaMemcpyAsync(out, in.buf[in.cur ^ 1], sizeof(T) * 5 * (size_t)in.p.nx * in.p.ny,
+                                  cudaMemcpyDeviceToHost, copy_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(copy_);
+  return e == cudaSuccess ? LE2D_OK : LE2D_ECUDA;
+}
+
+template <typename T>
+int Engine<T>::harvest_receivers(int id, T* out, int* nsamples) {
+  if (id < 0 || id >= (int)insts_.size()) return LE2D_EINVAL;
+  const Inst& in = insts_[id];
+  if (!in.live || in.failed) return in.failed ? LE2D_ETIMEOUT : LE2D_ESTATE;
+  const int have = in.trace ? (int)std::min<long long>(in.nsamples, in.done_steps / in.p.receiver_every) : 0;
+  if (nsamples) *nsamples = have;
+  if (!out || have == 0) return LE2D_OK;
+  cudaError_t e = cudaMemcpy2DAsync(out, sizeof(T) * in.p.nx, in.trace, sizeof(T) * in.pitch,
+                                    sizeof(T) * in.p.nx, 2 * (size_t)have, cudaMemcpyDeviceToHost, copy_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(copy_);
+  return e == cudaSuccess ? LE2D_OK : LE2D_ECUDA;
+}
+
+template <typename T>
 int Engine<T>::fields(int id, T* out) {
   if (id < 0 || id >= (int)insts_.size() || !out) return LE2D_EINVAL;
   const Inst& in = insts_[id];
   if (!in.live) return LE2D_ESTATE;
+  if (in.failed) return LE2D_ETIMEOUT;
   const int cur = in.cur;
   cudaError_t e = launch_unpack<T>(in.buf[cur], in.buf[cur ^ 1], in.p.nx, in.p.ny, in.pitch,
                                    in.plane, in.p.stype == ST_AOS, stream_);
@@ -552,6 +725,7 @@ int Engine<T>::receivers(int id, T* out, int* nsamples) {
   if (id < 0 || id >= (int)insts_.size()) return LE2D_EINVAL;
   const Inst& in = insts_[id];
   if (!in.live) return LE2D_ESTATE;
+  if (in.failed) return LE2D_ETIMEOUT;
   const int have = in.trace ? (int)std::min<long long>(in.nsamples, in.done_steps / in.p.receiver_every) : 0;
   if (nsamples) *nsamples = have;
   if (!out || have == 0) return LE2D_OK;
@@ -567,6 +741,7 @@ int Engine<T>::diagnostics(int id, le2d_diag_t* out) {
   if (id < 0 || id >= (int)insts_.size() || !out || !d_diag_) return LE2D_EINVAL;
   const Inst& in = insts_[id];
   if (!in.live) return LE2D_ESTATE;
+  if (in.failed) return LE2D_ETIMEOUT;
   const double rho = in.p.rho, c1 = in.p.c1, c2 = in.p.c2;
   const double mu = rho * c2 * c2, la = rho * c1 * c1 - 2.0 * mu;
   double h[11];

@@ -51,6 +51,12 @@ class Engine {
     StepConsts<T> c;
     int nstrips = 0, nsegs = 0, seg_len = 0;
     bool live = false;
+    int* fail = nullptr;     // failure word on the device (in the instance's arena block)
+    bool failed = false;     // a dependency wait of one of its tiles gave up: no results
+    bool prologue = false;   // initial condition still to be applied (add_async)
+    bool has_init = false;   //   from the host state uploaded into buf[1]
+    std::vector<T> disks;    //   or from these disks (4 values each)
+    bool unpacked = false;   // final fields unpacked into buf[cur ^ 1] after its last window
   };
 
   explicit Engine(size_t budget_bytes);
@@ -62,17 +68,37 @@ class Engine {
   static size_t footprint(const le2d_problem& p);
   // Validates, allocates and initialises an instance; returns its id or -LE2D_E*.
   int add(const le2d_problem& p, const T* init, int ndisks, const T* disks);
-  // Advances every live instance with steps left by min(left, window) steps in one
-  // persistent launch (not captured); returns LE2D_OK / LE2D_ETIMEOUT / LE2D_ECUDA.
+  // The same, for use while a window is in flight: allocates the instance and copies the
+  // host initial state `init` into its second buffer on the copy stream (the call returns
+  // once `init` has been read); the initial condition is applied on the step stream just
+  // before the next window, so no kernel competes with the window for the SMs.
+  int add_async(const le2d_problem& p, const T* init, int ndisks, const T* disks);
+  // One window: every live instance with steps left advances by min(left, window) steps
+  // in one persistent launch (not captured).  begin_window() applies pending initial
+  // conditions, launches and returns; after the launch it also queues, on the step
+  // stream, the unpacking of the final fields of the instances the window finishes.
+  // end_window() waits for it: LE2D_OK (instances whose dependency wait gave up are
+  // marked failed()), LE2D_ETIMEOUT (a wait inside a warp pair gave up: every instance
+  // of the window failed) or LE2D_ECUDA.
+  int begin_window(int window);
+  int end_window();
+  bool in_flight() const { return in_flight_; }
+  // begin_window + end_window.
   int run_window(int window);
   // Runs every live instance to completion: all windows captured in one CUDA graph.
+  // LE2D_ETIMEOUT if an instance failed (the others' results are valid).
   int run_all(int window, float* ms);
   int fields(int id, T* out);
   int receivers(int id, T* out, int* nsamples);
+  // Results of an instance finished by an earlier window, read on the copy stream, so
+  // they overlap a window in flight (fields: unpacked after the finishing window).
+  int harvest_fields(int id, T* out);
+  int harvest_receivers(int id, T* out, int* nsamples);
   int diagnostics(int id, le2d_diag_t* out);
   // Releases the instance's device memory (its results must have been read).
   void release(int id);
   bool finished(int id) const;
+  bool failed(int id) const;
   int count() const { return (int)insts_.size(); }
   const Inst& inst(int id) const { return insts_[id]; }
   void set_wait_ns(unsigned long long ns) { wait_ns_ = ns; }
@@ -102,11 +128,19 @@ class Engine {
   int launch_window(const Window& w, size_t inst_off, size_t tile_off, size_t item_off,
                     size_t done_off, size_t ctl_off);
 
+  int apply_prologues();  // pending initial conditions, on the step stream
+  int alloc_instance(const le2d_problem& p, Inst& in);
+  int read_failures(const std::vector<int>& ids);
+
   Arena* arena_ = nullptr;
   cudaStream_t stream_ = nullptr;
+  cudaStream_t copy_ = nullptr;  // uploads and read-backs beside a window
+  Window win_;                   // the window in flight
+  bool in_flight_ = false;
   std::vector<Inst> insts_;
   unsigned long long wait_ns_ = 2000000000ULL;
-  int stall_tile_ = -1;  // test hook from LE2D_TEST_STALL_TILE (see launch_batch)
+  int stall_tile_ = -1;  // test hook from LE2D_TEST_STALL_TILE (see launch_batch): in the
+                         // engine's first window only
   int seg_len_ = 64;
   bool seg_set_ = false;
   int depth_set_ = 0;

@@ -106,6 +106,8 @@ struct BatchInst {
   T* trace;              // receiver samples [sample][2][pitch], or null
   int trace_row;         // receiver row
   int trace_every;       // steps between samples
+  int* fail;             // the instance's failure word (0 = ok); set when a wait of one of
+                         // its tiles gives up, after which its work items are skipped
 };
 
 struct BatchTile {
@@ -114,8 +116,10 @@ struct BatchTile {
 
 struct BatchCtl {
   unsigned long long next;  // next work item
-  int status;               // 0 = ok, 1 = a dependency wait gave up
-  int pad;
+  int status;               // 0 = ok, 1 = a wait between the warps of a pair gave up: the
+                            // launch ends early and no instance of it has valid results
+  int failed;               // instances whose failure word this launch set (a dependency
+                            // wait gave up; only those instances are affected)
 };
 
 template <typename T>

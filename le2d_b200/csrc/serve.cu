@@ -4,14 +4,20 @@
 // Clients call le2d_server_submit from any thread; the request (problem, initial
 // condition) is copied into a ticket and queued.  The worker repeats:
 //   1. admit queued requests, in arrival order, while the engine's arena can hold
-//      their states (the HBM budget) and fewer than max_active run; a request that
-//      cannot fit even into an empty arena fails with LE2D_EBUDGET;
-//   2. advance every admitted solve by up to window_steps steps in one persistent
-//      launch (solves of different sizes and materials share the launch);
-//   3. move finished solves' results (final fields or receiver traces) into their
-//      tickets, free their device memory and wake the waiters.
-// So requests that arrive while others are on the GPU join at the next window and
-// their work overlaps with the others'.
+//      their states (the HBM budget) and fewer than max_active run; their initial
+//      states go to the device on a copy stream, beside the window in flight;
+//   2. wait for the window in flight, if any;
+//   3. launch the next window: every admitted solve with steps left advances by up to
+//      window_steps steps in one persistent launch (solves of different sizes and
+//      materials share it); the final fields of the solves it finishes are unpacked
+//      right after it;
+//   4. while that window runs, read back the results (final fields or receiver traces)
+//      of the solves the previous window finished, on the copy stream, free their
+//      device memory and wake the waiters.
+// So requests that arrive while others are on the GPU join at the next window, their
+// work overlaps with the others', and uploads and read-backs overlap the windows.  A
+// solve whose tiles' dependency wait gave up fails alone (LE2D_ETIMEOUT); a launch that
+// ended early fails the solves it carried.
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -74,74 +80,110 @@ struct le2d_server {
 
   void run() {
     std::unique_lock<std::mutex> lk(mu);
-    while (!stop) {
-      // 1. admission against the arena (HBM budget)
-      while (!queue.empty() && (int)active.size() < max_active) {
+    double t_launch = 0.0;
+    long long nu_launch = 0;
+    while (true) {
+      // 1. admission against the arena (HBM budget); the engine calls run unlocked
+      std::vector<std::shared_ptr<Ticket>> cand;
+      while (!stop && !queue.empty() && (int)(active.size() + cand.size()) < max_active) {
         auto it = tickets.find(queue.front());
-        if (it == tickets.end()) {
-          queue.pop_front();
-          continue;
-        }
-        std::shared_ptr<Ticket> t = it->second;
-        const int id = eng->add(t->p, t->init.empty() ? nullptr : t->init.data(),
-                                (int)(t->disks.size() / 4), t->disks.empty() ? nullptr : t->disks.data());
-        if (id == -LE2D_EBUDGET && !active.empty()) break;  // wait for memory to free up
         queue.pop_front();
-        if (id < 0) {
-          finish(t, id);
-          cv_done.notify_all();
+        if (it != tickets.end()) cand.push_back(it->second);
+      }
+      const bool busy = !active.empty() || eng->in_flight();
+      lk.unlock();
+      std::vector<std::pair<std::shared_ptr<Ticket>, int>> added;  // ticket, engine id or -error
+      size_t k = 0;
+      for (; k < cand.size(); ++k) {
+        const auto& t = cand[k];
+        const int id = eng->add_async(t->p, t->init.empty() ? nullptr : t->init.data(),
+                                      (int)(t->disks.size() / 4), t->disks.empty() ? nullptr : t->disks.data());
+        if (id == -LE2D_EBUDGET && (busy || !added.empty())) break;  // wait for memory to free up
+        added.push_back({t, id});
+      }
+      lk.lock();
+      for (size_t j = cand.size(); j > k; --j) queue.push_front(cand[j - 1]->id);
+      const double t_adm = now_s();
+      for (auto& a : added) {
+        if (a.second < 0) {
+          finish(a.first, a.second);
           continue;
         }
-        t->engine_id = id;
-        t->t_admit = now_s();
-        t->init.clear();
-        t->init.shrink_to_fit();
-        active.push_back(t);
+        a.first->engine_id = a.second;
+        a.first->t_admit = t_adm;
+        a.first->init.clear();
+        a.first->init.shrink_to_fit();
+        active.push_back(a.first);
         ++st.admitted;
       }
-      if (active.empty()) {
+      if (!added.empty()) cv_done.notify_all();
+      if (stop) break;
+      if (active.empty() && !eng->in_flight()) {
         cv_work.wait(lk, [&] { return stop || !queue.empty(); });
         continue;
       }
-      // 2. one window over every admitted solve (the lock is released meanwhile)
       lk.unlock();
-      const double t0 = now_s();
-      const long long nu0 = eng->node_updates();
-      const int rc = eng->run_window(window);
-      const double t1 = now_s();
-      lk.lock();
-      st.device_busy_s += t1 - t0;
-      st.node_updates += eng->node_updates() - nu0;
-      ++st.windows;
-      // 3. harvest
-      std::vector<std::shared_ptr<Ticket>> keep;
-      for (auto& t : active) {
-        if (rc != LE2D_OK) {
-          eng->release(t->engine_id);
-          finish(t, -rc);
-          continue;
-        }
-        if (!eng->finished(t->engine_id)) {
-          keep.push_back(t);
-          continue;
-        }
-        int r2 = LE2D_OK;
-        if (t->want == LE2D_WANT_RECEIVERS) {
-          int n = 0;
-          r2 = eng->receivers(t->engine_id, nullptr, &n);
-          t->result.resize((size_t)n * 2 * t->p.nx);
-          t->nsamples = n;
-          if (r2 == LE2D_OK && n > 0) r2 = eng->receivers(t->engine_id, t->result.data(), &n);
-        } else {
-          t->result.resize((size_t)5 * t->p.nx * t->p.ny);
-          r2 = eng->fields(t->engine_id, t->result.data());
-        }
-        eng->release(t->engine_id);
-        finish(t, r2 == LE2D_OK ? 1 : -r2);
+      // 2. the window in flight
+      int rc = LE2D_OK;
+      if (eng->in_flight()) {
+        rc = eng->end_window();
+        const double t1 = now_s();
+        std::lock_guard<std::mutex> g(mu);
+        st.device_busy_s += t1 - t_launch;
+        st.node_updates += eng->node_updates() - nu_launch;
+        ++st.windows;
       }
-      active.swap(keep);
-      cv_done.notify_all();
+      // 3. the next window
+      if (rc != LE2D_ECUDA) {
+        t_launch = now_s();
+        nu_launch = eng->node_updates();
+        rc = eng->begin_window(window);
+        if (rc == LE2D_ETIMEOUT) rc = LE2D_OK;  // per-solve failures are read below
+      }
+      // 4. results of the solves that are done, read beside the new window
+      std::vector<std::pair<std::shared_ptr<Ticket>, int>> done;  // ticket, final status
+      for (auto& t : active) {
+        const int id = t->engine_id;
+        int status = 0;
+        if (rc == LE2D_ECUDA) {
+          status = -LE2D_ECUDA;
+        } else if (eng->failed(id)) {
+          status = -LE2D_ETIMEOUT;
+        } else if (eng->finished(id)) {
+          int r2 = LE2D_OK;
+          if (t->want == LE2D_WANT_RECEIVERS) {
+            int n = 0;
+            r2 = eng->harvest_receivers(id, nullptr, &n);
+            t->result.resize((size_t)n * 2 * t->p.nx);
+            t->nsamples = n;
+            if (r2 == LE2D_OK && n > 0) r2 = eng->harvest_receivers(id, t->result.data(), &n);
+          } else {
+            t->result.resize((size_t)5 * t->p.nx * t->p.ny);
+            r2 = eng->harvest_fields(id, t->result.data());
+          }
+          status = r2 == LE2D_OK ? 1 : -r2;
+        }
+        if (status != 0) {
+          eng->release(id);
+          done.push_back({t, status});
+        }
+      }
+      lk.lock();
+      if (!done.empty()) {
+        std::vector<std::shared_ptr<Ticket>> keep;
+        for (auto& t : active) {
+          bool fin = false;
+          for (auto& d : done) fin = fin || d.first == t;
+          if (!fin) keep.push_back(t);
+        }
+        for (auto& d : done) finish(d.first, d.second);
+        active.swap(keep);
+        cv_done.notify_all();
+      }
     }
+    lk.unlock();
+    if (eng->in_flight()) eng->end_window();
+    lk.lock();
     for (auto& t : active) eng->release(t->engine_id);
     active.clear();
   }

@@ -26,6 +26,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD_DIR = os.path.join(HERE, "_build")
 REF_DIR = os.path.join(HERE, "_ref")
+# Where the reference project's sources are mounted (read-only): LE2D_REFERENCE, else the
+# mount point of this build environment.  Absent on machines that only run the prebuilt
+# oracle/_ref libraries.
+REFERENCE_ROOT = os.environ.get("LE2D_REFERENCE", "/root/reference")
 
 ST_SOA = 0
 ST_AOS = 1
@@ -35,7 +39,7 @@ _I = ctypes.c_int
 _D = ctypes.c_double
 
 
-def build(reference_root: str | None = "/root/reference") -> None:
+def build(reference_root: str | None = REFERENCE_ROOT) -> None:
     """Compile the restatement and, when the reference sources exist, oracle/_ref."""
     cmd = ["make", "-s", "-C", HERE, "oracle"]
     subprocess.run(cmd, check=True)

@@ -10,10 +10,11 @@ import tempfile
 import pytest
 
 from le2d_b200 import capi
+from oracle.oracle import REFERENCE_ROOT
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INCLUDE = os.path.join(ROOT, "include")
-REF = "/root/reference"
+REF = REFERENCE_ROOT
 
 
 def header_functions():

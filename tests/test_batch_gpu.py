@@ -135,22 +135,33 @@ def test_batch_budget_and_validation(libs):
         assert b.run()[0] == 0
 
 
-def test_batch_bounded_wait_gives_up(libs, monkeypatch):
-    """A tile that never publishes its first step (test hook): the waits that depend on it
-    run out after the wait limit, the run reports LE2D_ETIMEOUT, the device stays usable."""
-    lib = libs["f"]
-    p = workloads.Problem(300, 200, 1, 1, 2, 1, 1, 0.25, 6, [(150.0, 100.0, 30.0, 1.0)])
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_batch_bounded_wait_gives_up(libs, prec, monkeypatch):
+    """A tile that never publishes its first step (test hook, first tile of the first
+    window): the waits that depend on it run out after the wait limit and its instance
+    fails alone -- le2d_batch_run reports LE2D_ETIMEOUT, the instance's results report
+    LE2D_ETIMEOUT, the other instances' results equal their solves alone, and the device
+    stays usable."""
+    lib = libs[prec]
+    victim = workloads.Problem(300, 200, 1, 1, 2, 1, 1, 0.25, 6, [(150.0, 100.0, 30.0, 1.0)])
+    others = small_set(41, 3, 20, 200, 2, 5)  # fewer steps: ordered after the victim
     monkeypatch.setenv("LE2D_TEST_STALL_TILE", "0")
     with capi.Batch(lib, 1 << 28) as b:
         assert b.set_wait_limit(50_000_000) == 0  # 50 ms
-        b.add(b.problem(p), disks=p.disks)
+        iv = b.add(b.problem(victim), disks=victim.disks)
+        ids = [b.add(b.problem(p), disks=p.disks) for p in others]
         rc, _ = b.run(window_steps=6)
         assert rc == capi.LE2D_ETIMEOUT
+        out = np.zeros(5 * victim.nx * victim.ny, lib.dtype)
+        assert lib.lib.le2d_batch_fields(b.h, iv, out.ctypes.data) == capi.LE2D_ETIMEOUT
+        for i, p in zip(ids, others):
+            want, _ = solve_alone(lib, p, ST_AOS)
+            assert b.fields(i).tobytes() == want.tobytes()
     monkeypatch.delenv("LE2D_TEST_STALL_TILE")
     with capi.Batch(lib, 1 << 28) as b:  # a normal run afterwards
-        i = b.add(b.problem(p), disks=p.disks)
+        i = b.add(b.problem(victim), disks=victim.disks)
         assert b.run()[0] == 0
-        want, _ = solve_alone(lib, p, ST_AOS)
+        want, _ = solve_alone(lib, victim, ST_AOS)
         assert b.fields(i).tobytes() == want.tobytes()
 
 

@@ -32,15 +32,20 @@ def test_mix_equals_alone(lib):
             st = ST_SOA if k % 4 == 3 else ST_AOS
             tickets.append((srv.submit(srv_problem(lib, p, st), disks=p.disks), p, st))
             time.sleep(0.002 * (k % 3))
+        spans = []
         for t, p, st in tickets:
             assert t > 0
             assert srv.wait(t, 60.0) == 0
             got = srv.result(t)
             want, _ = solve_alone(lib, p, st)
             assert got.tobytes() == want.tobytes(), (p.nx, p.ny, p.steps, st)
+            spans.append(srv.times(t))
         s = srv.stats()
         assert s["completed"] == len(probs) and s["failed"] == 0
         assert s["windows"] >= 2
+        # continuous batching: some request was admitted while another was on the device
+        joined = [b for b in spans for a in spans if a is not b and a[1] < b[1] < a[2]]
+        assert joined, spans
 
 
 def srv_problem(lib, p, stype=ST_AOS, receiver_row=-1, every=10):
@@ -108,3 +113,22 @@ def test_concurrent_submitters(lib):
     for p in probs:
         want, _ = solve_alone(lib, p, ST_AOS)
         assert results[id(p)].tobytes() == want.tobytes()
+
+
+def test_failed_solve_fails_alone(lib, monkeypatch):
+    """A solve whose device work stalls (test hook: the first tile of the server's first
+    window never publishes) fails with LE2D_ETIMEOUT after the bounded wait; the requests
+    beside it complete and equal their solves alone."""
+    monkeypatch.setenv("LE2D_TEST_STALL_TILE", "0")
+    victim = workloads.Problem(300, 200, 1, 1, 2, 1, 1, 0.25, 40, [(150.0, 100.0, 30.0, 1.0)])
+    others = small_set(34, 5, 16, 120, 4, 7)  # fewer steps than the window: ordered after the victim
+    with capi.Server(lib, 1 << 28, window_steps=8) as srv:
+        tv = srv.submit(srv_problem(lib, victim), disks=victim.disks)
+        ts = [srv.submit(srv_problem(lib, p), disks=p.disks) for p in others]
+        assert srv.wait(tv, 60.0) == capi.LE2D_ETIMEOUT
+        for t, p in zip(ts, others):
+            assert srv.wait(t, 60.0) == 0
+            want, _ = solve_alone(lib, p, ST_AOS)
+            assert srv.result(t).tobytes() == want.tobytes()
+        s = srv.stats()
+        assert s["failed"] == 1 and s["completed"] == len(others)

@@ -10,6 +10,9 @@ tolerance the diagnostics tests use (1e-12 relative on the sums, exact on the ma
 This file is collected last so that a failure here leaves every other test run.
 """
 import ctypes
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -72,3 +75,47 @@ def test_noalloc_rejects_too_many_rows():
     # rejected by the host-side size check before any device work
     rc, _ = lib.diagnostics_noalloc(256, 8, ny, 8, 8 * ny, 1.0, 1.0, 2.0, 1.0, 1.0)
     assert rc == capi.LE2D_EINVAL
+
+
+# Run in a child process: it resets the device, which ends every context of the process.
+_RESET_SCRIPT = r"""
+import ctypes, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from le2d_b200 import capi
+from oracle.oracle import ST_AOS, Oracle, aos_to_soa
+prec = sys.argv[2]
+lib, o = capi.Lib(prec), Oracle(prec)
+rt = ctypes.CDLL("libcudart.so")
+rt.cudaMalloc.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t]
+rt.cudaFree.argtypes = [ctypes.c_void_p]
+rt.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+nx, ny = 257, 131
+for rnd in range(2):
+    g = np.random.default_rng(rnd).uniform(-1, 1, 5 * nx * ny).astype(o.dtype)
+    want = o.diag(g, nx, ny, 1.0, 1.0, 2.0, 1.0, 1.5, ST_AOS)
+    soa = aos_to_soa(g, nx, ny)
+    d = ctypes.c_void_p()
+    assert rt.cudaMalloc(ctypes.byref(d), soa.nbytes) == 0
+    assert rt.cudaMemcpy(d, soa.ctypes.data, soa.nbytes, 1) == 0
+    rc, got = lib.diagnostics_noalloc(d.value, nx, ny, nx, nx * ny, 1.0, 1.0, 2.0, 1.0, 1.5)
+    assert rc == 0, lib.strerror(rc)
+    assert abs(got["energy"] - want[0]) <= 1e-12 * abs(want[0]), (rnd, got["energy"], want[0])
+    assert np.allclose(got["sumsq"], want[1:6], rtol=1e-12, atol=0), rnd
+    assert got["maxabs"] == list(want[6:11]), rnd
+    assert rt.cudaFree(d) == 0
+    if rnd == 0:
+        assert rt.cudaDeviceReset() == 0  # a new context: the cached scratch address is stale
+print("ok")
+"""
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_noalloc_after_device_reset(prec):
+    """A caller that resets the device (cudaDeviceReset) between two calls: the second call
+    looks the scratch array's address up again in the new context and is still correct
+    (against the oracle's diagnostics of the same state)."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _RESET_SCRIPT, root, prec], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
