@@ -614,6 +614,80 @@ def run_slabs(args):
     return 0
 
 
+def run_parity(args):
+    """The 8192x8192 workload at its full length (1000 steps) through the library, FP32 and
+    FP64, against the reference's own simple/ float and double builds (oracle/_ref, OpenMP;
+    the two builds run side by side on half the host threads each): per-field relative L2
+    and max-abs, and whether the FP64 result equals the reference double build's."""
+    import threading
+
+    from oracle.oracle import ST_AOS, Oracle, Reference, fields, max_abs, rel_l2
+
+    p = workloads.single_8192() if args.time_steps is None else workloads.single_8192(args.time_steps)
+    n = p.nx
+    ours, t_gpu = {}, {}
+    for prec in ("f", "d"):
+        lib = capi.Lib(prec)
+        t = new_task(lib, p)
+        try:
+            initial_state(lib, p, t)
+            rc, ms = lib.step_n_timed(t, p.steps)
+            assert rc == 0, lib.strerror(rc)
+            g = np.zeros(5 * p.nodes, lib.dtype)
+            assert lib.download(t, g) == 0 and lib.last_error(t) == 0
+            ours[prec], t_gpu[prec] = g, ms * 1e-3
+        finally:
+            lib.le_free_task(t)
+    threads = os.cpu_count() or 2
+    refs, secs = {}, {}
+    if Reference.available("d"):
+        kind = "reference simple/ (oracle/_ref, gcc -O2 -fno-tree-vectorize, OpenMP)"
+
+        def ref_run(prec, thr):
+            o = Oracle(prec)
+            g = np.zeros(5 * p.nodes, o.dtype)
+            for cx, cy, r, s_ in p.disks:
+                o.set_ball(g, n, n, p.hx, p.hy, ST_AOS, cx, cy, r, s_)
+            secs[prec] = Reference(prec).run(g, n, n, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, ST_AOS, p.steps, thr)
+            refs[prec] = g
+
+        th = [threading.Thread(target=ref_run, args=(q, max(1, threads // 2))) for q in ("f", "d")]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+    else:
+        kind = "unavailable (oracle/_ref not built)"
+    line = {"metric": "parity", "workload": f"single_8192: {n}x{n}, {p.steps} time steps, 8 seeded disks",
+            "gpu_seconds": t_gpu, "reference": kind, "reference_threads_each": max(1, threads // 2),
+            "reference_seconds": secs}
+    if refs:
+        fo = {q: fields(ours[q], n, n, ST_AOS) for q in ("f", "d")}
+        fr = {q: fields(refs[q], n, n, ST_AOS) for q in ("f", "d")}
+        line.update({
+            "fp64_equal_to_reference_double": bool(np.array_equal(ours["d"], refs["d"])),
+            "fp64_vs_reference_double_rel_l2": rel_l2(fo["d"], fr["d"]).tolist(),
+            "fp64_vs_reference_double_max_abs": max_abs(fo["d"], fr["d"]).tolist(),
+            "fp32_vs_reference_float_rel_l2": rel_l2(fo["f"], fr["f"]).tolist(),
+            "fp32_vs_reference_double_rel_l2": rel_l2(fo["f"], fr["d"]).tolist(),
+            "fp32_vs_reference_double_max_abs": max_abs(fo["f"], fr["d"]).tolist(),
+            "reference_float_vs_double_rel_l2": rel_l2(fr["f"], fr["d"]).tolist(),
+            "tolerances": {"fp64": 1e-12, "fp32": 1e-5},
+        })
+        # FP32: 1e-5 per field, or -- the tests' rule -- 4x the reference float build's own
+        # distance from its double build where that is larger
+        gap = np.array(line["reference_float_vs_double_rel_l2"])
+        tol = np.maximum(1e-5, 4.0 * gap)
+        line["pass_fp64"] = bool(max(line["fp64_vs_reference_double_rel_l2"]) <= 1e-12)
+        line["pass_fp32_1e-5"] = bool(max(line["fp32_vs_reference_float_rel_l2"]) <= 1e-5 and
+                                      max(line["fp32_vs_reference_double_rel_l2"]) <= 1e-5)
+        line["pass_fp32_with_float_build_allowance"] = bool(
+            np.all(np.array(line["fp32_vs_reference_float_rel_l2"]) <= tol) and
+            np.all(np.array(line["fp32_vs_reference_double_rel_l2"]) <= tol))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_precision(args):
     """4096x4096 precision study: FP32 vs FP64 library every 500 steps up to 4000 steps,
     FP64 energy drift, and both builds against the reference's own CPU builds after 500 steps."""
@@ -723,7 +797,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="single",
-                    choices=["single", "batched", "serving", "precision", "precision-reference", "slabs"])
+                    choices=["single", "batched", "serving", "precision", "precision-reference", "slabs",
+                             "parity"])
     ap.add_argument("--slabs", default="2,4", help="slabs: slab counts besides the whole task")
     ap.add_argument("--window", type=int, default=256, help="steps per persistent launch (batched/serving)")
     ap.add_argument("--rates", default="10,50,200,2000", help="serving: request rates per second")
@@ -749,6 +824,8 @@ def main():
         return run_precision_reference(args)
     if args.workload == "slabs":
         return run_slabs(args)
+    if args.workload == "parity":
+        return run_parity(args)
 
     world, rank, local = dist_setup()
     backend = "nccl"

@@ -210,9 +210,12 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
         break;
     }
   } else {
+    // the producer hands over an item only after its dependency wait, which may run out
+    // (wait_ns) and hand over a skip instead: the consumer's wait for the item outlasts it
+    const unsigned long long item_wait_ns = wait_ns > ~0ULL / 4 ? ~0ULL : 4 * wait_ns;
     while (true) {
       const int hs = (int)(u % kHand);
-      if (!march::mbar_wait(bars + hs, (u / kHand) & 1, wait_ns, status)) break;
+      if (!march::mbar_wait(bars + hs, (u / kHand) & 1, item_wait_ns, status)) break;
       const long long q = item_q[hs];
       march::mbar_arrive(bars + kHand + hs);
       ++u;

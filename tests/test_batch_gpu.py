@@ -3,8 +3,9 @@
 The persistent batched kernel marches every tile with the same per-node operations
 as the single-solve kernel, so each instance's result must equal, bit for bit, the
 same instance solved alone with le_step; the single-solve path is itself checked
-against the reference (test_parity_gpu.py), and a few instances are also checked
-against the oracle here (FP32 <= 1e-5, FP64 <= 1e-12 relative L2 per field).
+against the reference (test_parity_gpu.py), and instances are also checked against the
+oracle and the reference here (FP32 <= 1e-5 relative L2 per field; FP64 <= 1e-12, and
+equal value for value on the instances drawn from the uneven mix).
 """
 import os
 
@@ -87,6 +88,48 @@ def test_batch_against_oracle(libs, prec):
             o.run(g, p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, ST_AOS, p.steps)
             err = rel_l2(got, fields(g, p.nx, p.ny, ST_AOS))
             assert np.all(err <= tol), (i, err)
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_batch_mix_subset_against_reference(libs, prec):
+    """16 instances drawn (seeded) from the 256-instance uneven mix itself -- sizes, materials,
+    disks and step counts as generated, among the instances of at most 5e7 node-updates so
+    the CPU side stays short -- in one batched run (default tiles), against the reference
+    solver run on the host (oracle/_ref: the reference's own simple/ build, OpenMP; else the
+    C oracle, which reproduces it bit for bit).  FP64: equal value for value.  FP32: within
+    1e-5 per field of the reference float and double builds, or 4x the float build's own
+    distance from its double build where that is larger (small boxes with many reflections)."""
+    from oracle.oracle import Reference
+    from test_parity_gpu import check
+
+    lib = libs[prec]
+    mix = workloads.batched_256()
+    small = [k for k, p in enumerate(mix) if p.node_updates <= 5e7]
+    pick = sorted(np.random.default_rng(16).choice(small, size=min(16, len(small)), replace=False))
+    threads = os.cpu_count() or 1
+    lib.batch_autotune_reset()
+    with capi.Batch(lib, 1 << 32) as b:
+        ids = [b.add(b.problem(mix[k]), disks=mix[k].disks) for k in pick]
+        assert b.run(window_steps=256)[0] == 0
+        for i, k in zip(ids, pick):
+            p = mix[k]
+            got = b.fields(i)
+            want = {}
+            for q in ("f", "d") if prec == "f" else ("d",):
+                o = Oracle(q)
+                g = np.zeros(5 * p.nx * p.ny, o.dtype)
+                for d in p.disks:
+                    o.set_ball(g, p.nx, p.ny, p.hx, p.hy, ST_AOS, *d)
+                if Reference.available(q):
+                    Reference(q).run(g, p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, ST_AOS, p.steps, threads)
+                else:
+                    o.run(g, p.nx, p.ny, p.dt, p.hx, p.hy, p.c1, p.c2, p.rho, ST_AOS, p.steps)
+                want[q] = g
+            if prec == "d":
+                assert np.array_equal(got, want["d"]), (k, p.nx, p.ny, p.steps)
+            else:
+                check("f", got, want["f"], want["d"], p.nx, p.ny, ST_AOS,
+                      f"mix[{k}] {p.nx}x{p.ny} x{p.steps}")
 
 
 def test_batch_init_arrays_and_receivers(libs):

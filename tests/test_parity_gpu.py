@@ -11,10 +11,12 @@ Tolerances (per field, relative L2 = ||a-b|| / ||b||):
     distance from its double build when that exceeds 1e-5/4.
 Max-abs error of every result against the FP64 reference is printed (pytest -s).
 """
+import hashlib
+
 import numpy as np
 import pytest
 
-from golden_cases import arrays, cases
+from golden_cases import arrays, cases, summary
 from le2d_b200 import capi, workloads
 from oracle.oracle import ST_AOS, ST_SOA, Oracle, aos_to_soa, fields, max_abs, rel_l2
 
@@ -89,6 +91,44 @@ def test_golden_case(libs, name, prec, method):
     got = run(libs[prec], c, a[f"{name}__in"], c["steps"], METHODS[method])
     check(prec, got, a[f"{name}__out"], ad[f"{name}__out"], c["nx"], c["ny"], c["stype"],
           f"{name}/{prec}/{method}")
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_plain_512_full_length(libs, prec):
+    """The reference driver's plain workload at its full length (512x512, c1=2, c2=1,
+    rho=1, dt=0.25, disk r=25 at the centre with s=1, 200 steps, AoS): one le_step call
+    per step as simple/main.c makes them.  FP64: the final grid hashes to the digest of the
+    reference double build's own output (tests/golden/golden.json, plain_512); FP32: within
+    1e-5 of the reference float and double builds (the C oracle, which reproduces both bit
+    for bit), max-abs against the double build printed."""
+    lib = libs[prec]
+    nx = ny = 512
+    c = dict(nx=nx, ny=ny, hx=1.0, hy=1.0, c1=2.0, c2=1.0, rho=1.0, dt=0.25, stype=ST_AOS)
+    t = make_task(lib, c)
+    try:
+        lib.le_set_ball(t, (256.0, 256.0), 25.0, 1.0)
+        for _ in range(200):
+            lib.le_step(t)
+        assert lib.sync_host(t) == 0 and lib.last_error(t) == 0
+        got = lib.grid_view(t).copy()
+    finally:
+        lib.le_free_task(t)
+    digest = summary()["plain_512"]
+    if prec == "d":
+        assert hashlib.sha256(got.tobytes()).hexdigest() == digest["d"]["sha256"]
+        print(f"\nplain_512/d: bytes equal to the reference double build's output")
+        return
+    want = {}
+    for q in ("f", "d"):
+        o = Oracle(q)
+        g = np.zeros(5 * nx * ny, o.dtype)
+        o.set_ball(g, nx, ny, 1.0, 1.0, ST_AOS, 256.0, 256.0, 25.0, 1.0)
+        o.run(g, nx, ny, 0.25, 1.0, 1.0, 2.0, 1.0, 1.0, ST_AOS, 200)
+        assert hashlib.sha256(g.tobytes()).hexdigest() == digest[q]["sha256"]  # the reference's bytes
+        want[q] = g
+    check("f", got, want["f"], want["d"], nx, ny, ST_AOS, "plain_512/f")
+    e = rel_l2(fields(got, nx, ny, ST_AOS), fields(want["d"], nx, ny, ST_AOS))
+    assert np.all(e <= TOL["f"]), e
 
 
 @pytest.mark.parametrize("prec", ["f", "d"])
