@@ -688,6 +688,62 @@ def run_parity(args):
     return 0
 
 
+def run_dist(args):
+    """The 8192x8192 solve as ONE grid split into row slabs, one rank per GPU (torchrun):
+    each rank steps its slab with the library and swaps the 4 owned rows beside each cut
+    with its neighbours through NCCL send/recv after every two steps (le2d_b200.dist_slabs).
+    Total work is fixed (strong scaling); value = the grid's node-updates / slowest rank."""
+    import torch
+
+    from le2d_b200.dist_slabs import GpuRankSlab
+
+    world, rank, local = dist_setup()
+    dist = dist_init(world, local, "nccl")
+    torch.cuda.set_device(local)
+    lib = capi.Lib("f")
+    assert lib.set_device(local) == 0
+    p = workloads.single_8192() if args.time_steps is None else workloads.single_8192(args.time_steps)
+    t = new_task(lib, p)
+    try:
+        ic = initial_state(lib, p, t).copy()
+    finally:
+        lib.le_free_task(t)
+    slab = GpuRankSlab(lib, dist, rank, world, p.nx, p.ny, p.dt, (p.hx, p.hy), p.c1, p.c2, p.rho)
+    try:
+        assert slab.upload(ic) == 0
+        for _ in range(args.warmup):
+            assert slab.step_n(8) == 0
+        assert slab.upload(ic) == 0 and lib.wait(slab.task) == 0
+        torch.cuda.synchronize()
+        dist_barrier(dist)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            assert slab.step_n(p.steps) == 0
+        assert lib.wait(slab.task) == 0
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        dist_barrier(dist)
+        slow = dist_max(dist, sec, "nccl")
+        rows = slab.x.own
+    finally:
+        slab.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank == 0:
+        nu = p.node_updates * args.steps
+        print(json.dumps({"metric": "node-updates/s", "value": nu / slow, "unit": "node-updates/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * slow / args.steps, "higher_is_better": True,
+                          "scaling": "strong", "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": f"dist: one {p.nx}x{p.ny} grid in {world} row slabs "
+                                                 f"(one per rank), {p.steps} time steps per bench step, "
+                                                 "4 halo rows swapped by NCCL send/recv every 2 steps",
+                                     "rows_rank0": rows},
+                          "timing": "host clock between device synchronisations, max over ranks"}),
+              flush=True)
+    return 0
+
+
 def run_precision(args):
     """4096x4096 precision study: FP32 vs FP64 library every 500 steps up to 4000 steps,
     FP64 energy drift, and both builds against the reference's own CPU builds after 500 steps."""
@@ -798,7 +854,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="single",
                     choices=["single", "batched", "serving", "precision", "precision-reference", "slabs",
-                             "parity"])
+                             "parity", "dist"])
     ap.add_argument("--slabs", default="2,4", help="slabs: slab counts besides the whole task")
     ap.add_argument("--window", type=int, default=256, help="steps per persistent launch (batched/serving)")
     ap.add_argument("--rates", default="10,50,200,2000", help="serving: request rates per second")
@@ -826,6 +882,8 @@ def main():
         return run_slabs(args)
     if args.workload == "parity":
         return run_parity(args)
+    if args.workload == "dist":
+        return run_dist(args)
 
     world, rank, local = dist_setup()
     backend = "nccl"

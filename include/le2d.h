@@ -221,6 +221,16 @@ int le2d_server_stats(le2d_server *s, le2d_server_stats_t *out);
 /* Host monotonic clock used by le2d_server_times (s). */
 double le2d_now(void);
 
+/* Rows [row0, row0 + nrows) of the task's current state copied to (rows_out) or from
+ * (rows_in) a device buffer of the caller, laid out [field][row][nx] (5 * nrows * nx reals),
+ * on the caller's CUDA stream `stream` (NULL = legacy default stream) and ordered with the
+ * task's own work both ways.  For a caller that exchanges boundary rows between processes
+ * itself (one process per GPU, e.g. NCCL send/recv on that stream): the rows a neighbour
+ * needs go out, its rows come in as halo rows.  New surface with no counterpart in the
+ * reference (whose multi-GPU variants copy rows within one process). */
+int le2d_rows_out(le_task *task, int row0, int nrows, real *dev_buf, void *stream);
+int le2d_rows_in(le_task *task, int row0, int nrows, const real *dev_buf, void *stream);
+
 /* Layout of the device state (SoA, 5 planes of n.y rows with a padded row pitch). */
 int le2d_device_layout(const le_task *task, long long *pitch_elems, long long *plane_elems);
 

@@ -49,6 +49,7 @@ EXPORTS = [
     "le2d_batch_autotune", "le2d_batch_autotune_reset",
     "le2d_slabs_create", "le2d_slabs_destroy", "le2d_slabs_rows", "le2d_slabs_upload",
     "le2d_slabs_download", "le2d_slabs_step_n", "le2d_slabs_wait", "le2d_selftest_ratio",
+    "le2d_rows_out", "le2d_rows_in",
 ]
 
 LE2D_DIAG_NOALLOC_MAX_ROWS = 16384
@@ -192,6 +193,8 @@ class Lib:
         L.le2d_slabs_download.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.le2d_slabs_step_n.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.le2d_slabs_wait.argtypes = [ctypes.c_void_p]
+        L.le2d_rows_out.argtypes = [P(self.le_task), ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.le2d_rows_in.argtypes = [P(self.le_task), ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.le2d_selftest_ratio.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
                                           ctypes.c_void_p, ctypes.c_void_p]
         L.le2d_diagnostics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
@@ -329,6 +332,14 @@ class Lib:
         rc = self.lib.le2d_diagnostics_noalloc(d_state, nx, ny, pitch, plane, hx, hy, c1, c2, rho,
                                                stream or None, ctypes.byref(d))
         return rc, {"energy": d.energy, "sumsq": list(d.sumsq), "maxabs": list(d.maxabs)}
+
+    def rows_out(self, t, row0: int, nrows: int, dev_ptr: int, stream: int = 0) -> int:
+        """Rows of the task's state into a device buffer [5][nrows][nx] (e.g. a CUDA tensor)."""
+        return self.lib.le2d_rows_out(ctypes.byref(t), row0, nrows, dev_ptr, stream or None)
+
+    def rows_in(self, t, row0: int, nrows: int, dev_ptr: int, stream: int = 0) -> int:
+        """Rows of the task's state from a device buffer [5][nrows][nx]."""
+        return self.lib.le2d_rows_in(ctypes.byref(t), row0, nrows, dev_ptr, stream or None)
 
     def device_layout(self, t):
         p, q = ctypes.c_longlong(0), ctypes.c_longlong(0)

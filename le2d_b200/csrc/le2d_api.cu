@@ -903,6 +903,53 @@ int le2d_diagnostics(le_task* task, le2d_diag_t* out) {
   return LE2D_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Rows [row0, row0 + nrows) of the task's state <-> a caller's device buffer laid out
+// [field][row][nx], on the caller's stream `stream`, ordered with the task's stream both ways
+// (events), so a caller can hand the rows to a collective on its own stream.
+int copy_rows(le_task* task, int row0, int nrows, T* dev_buf, void* stream, bool out) {
+  DevTask* d = lookup_sync(task);
+  if (!d) return LE2D_ENOTASK;
+  const char* what = out ? "le2d_rows_out" : "le2d_rows_in";
+  if (!dev_buf || nrows < 0 || row0 < 0 || row0 + nrows > d->ny) return record(d, LE2D_EINVAL, what);
+  int rc = ensure_device_current(d, task);
+  if (rc) return rc;
+  if (nrows == 0) return LE2D_OK;
+  const cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaEventRecord(d->ev[0], d->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, d->ev[0], 0);
+  for (int k = 0; k < 5 && e == cudaSuccess; ++k) {
+    T* state = d->buf[d->cur] + k * d->plane + (long long)row0 * d->pitch;
+    T* flat = dev_buf + (size_t)k * nrows * d->nx;
+    if (out)
+      e = cudaMemcpy2DAsync(flat, sizeof(T) * d->nx, state, sizeof(T) * d->pitch, sizeof(T) * d->nx, nrows,
+                            cudaMemcpyDeviceToDevice, s);
+    else
+      e = cudaMemcpy2DAsync(state, sizeof(T) * d->pitch, flat, sizeof(T) * d->nx, sizeof(T) * d->nx, nrows,
+                            cudaMemcpyDeviceToDevice, s);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(d->ev[1], s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(d->stream, d->ev[1], 0);
+  if (e != cudaSuccess) return record(d, LE2D_ECUDA, what, e);
+  if (!out) d->dev_newer = true;
+  return LE2D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int le2d_rows_out(le_task* task, int row0, int nrows, real* dev_buf, void* stream) {
+  return copy_rows(task, row0, nrows, dev_buf, stream, true);
+}
+
+int le2d_rows_in(le_task* task, int row0, int nrows, const real* dev_buf, void* stream) {
+  return copy_rows(task, row0, nrows, const_cast<real*>(dev_buf), stream, false);
+}
+
 int le2d_device_layout(const le_task* task, long long* pitch_elems, long long* plane_elems) {
   DevTask* d = lookup(task);
   if (!d) return LE2D_ENOTASK;

@@ -60,6 +60,15 @@ cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pi
                               long long plane, const StepConsts<T>& c, int far_rot,
                               const FusedPlan& plan, const PairCtl& pair, cudaStream_t s);
 
+// The same launch writing only some rows: `nranges` (1 or 2) row ranges [lo[r], hi[r]) of
+// the ny-row grid, cut into segments of seg_len rows; rows outside them are read (as the
+// stencil needs) but not written.
+template <typename T>
+cudaError_t launch_fused_rows(const T* src, T* dst, int nx, int ny, long long pitch, long long plane,
+                              const StepConsts<T>& c, int far_rot, const FusedPlan& plan,
+                              const PairCtl& pair, int seg_len, int nranges, const int* lo,
+                              const int* hi, cudaStream_t s);
+
 // The plain scheme: one sweep (axis 0 = x, 1 = y) src -> dst, one thread per node, the
 // reference's tvd2 formula node by node (two divisions per invariant).
 template <typename T>

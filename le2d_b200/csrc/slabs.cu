@@ -1,21 +1,28 @@
 // One grid split into row slabs over several devices (the reference's multi-GPU scheme,
 // le2d cuda5/cuda6: le_core.cu:374-509, one process driving every device with peer
-// copies of the rows next to each cut).
+// copies of the rows next to each cut; the copies overlapped with the interior, as
+// cuda6/le_core.cu:456-482 overlaps them with its y-sweep).
 //
 // Slab s owns the global rows [r0, r1) and keeps a copy of kHalo rows on each side that
 // has a neighbour (none at the grid's top and bottom), so its device grid is the rows
-// [r0 - h0, r1 + h1).  Every launch advances each slab with the unmodified fused kernel on
-// its own grid: at a cut that grid's clamped end is wrong, but the error enters two rows per
-// step, so after a launch of up to two steps the halo rows are spoiled and the owned rows
-// are exact.  The halo rows are then refreshed from the neighbours' owned rows (5 fields x
-// kHalo rows each way per cut, cudaMemcpy2DAsync between the devices' memories).  The
-// results are therefore bitwise those of the whole grid stepped by one task.
+// [r0 - h0, r1 + h1).  A launch advances a slab by up to two steps with the unmodified
+// fused kernels, writing only its owned rows: the stencil of two steps reaches 4 rows, so
+// the owned rows come out exact from the owned and halo rows of the launch before.
 //
-// Ordering.  Each slab has a stream on its device.  A launch of slab s is queued after its
-// own halo copies (same stream); a halo copy into slab s waits (event) for the launch of the
-// neighbour it reads from.  The neighbour's next launch, which overwrites the other buffer,
-// is queued after its own copies, which wait for slab s's launch; so no copy reads a buffer
-// that is being written and no launch overwrites rows a copy has not read yet.
+// Per launch and slab, in this order of dependencies:
+//   band     the owned rows beside each cut (4 each), on a high-priority stream, after
+//            the slab's previous interior and the halo copies into the slab;
+//   copies   each band's rows into the neighbour's halo rows (5 fields x 4 rows per cut
+//            and direction, cudaMemcpy2DAsync between the devices' memories), on the
+//            receiving slab's high-priority stream, after the sending slab's band;
+//   interior the other owned rows, on the slab's main stream, after its previous band.
+// So the copies and the next bands run while the interior rows are computed, and the
+// halo rows are never computed (they are copied).  Hazards: a band reads halo and owned
+// rows its previous interior and the copies wrote; an interior reads the owned rows its
+// previous band wrote, and overwrites rows that band read; a copy reads band rows that the
+// sender's next band overwrites only after the receiver's band, which follows the copy
+// on the receiver's stream, and after the copy back into the sender that waits for it.
+// The results are bitwise those of the whole grid stepped by one task.
 //
 // le_step_soa's far end (the last two rows read rows ny-5 and ny-4 instead of copies of row
 // ny-1) only affects the rows next to a grid's bottom: at a cut those are halo rows, and at
@@ -50,15 +57,17 @@ struct Slab {
   T* mem = nullptr;
   T* buf[2] = {nullptr, nullptr};
   int* d_status = nullptr;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev = nullptr;  // after this slab's last launch
+  cudaStream_t stream = nullptr;   // interior rows
+  cudaStream_t bstream = nullptr;  // boundary bands and the halo copies into this slab (high priority)
+  cudaEvent_t ev_band[2] = {nullptr, nullptr};  // after the band of launch k (k & 1)
+  cudaEvent_t ev_int[2] = {nullptr, nullptr};   // after the interior of launch k (k & 1)
   FusedPlan plan, plan1;
 };
 
 // Variant of each launch: FP32 two steps on warp pairs (one-step variant 2 for odd
-// remainders and SoA), FP64 one step (variant 15), as for whole tasks.
-int two_step_variant() { return sizeof(T) == 4 ? 13 : 15; }
-int one_step_variant() { return sizeof(T) == 4 ? 2 : 15; }
+// remainders and SoA), FP64 one step (variant 14), as for whole tasks.
+int two_step_variant() { return sizeof(T) == 4 ? 13 : 14; }
+int one_step_variant() { return sizeof(T) == 4 ? 2 : 14; }
 
 }  // namespace
 
@@ -68,6 +77,7 @@ struct le2d_slabs {
   StepConsts<T> c;
   std::vector<Slab> s;
   int cur = 0;  // buffer holding the state (the same on every slab)
+  long long launches = 0;
   int err = LE2D_OK;
 
   int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
@@ -89,25 +99,26 @@ cudaError_t copy_rows(le2d_slabs* S, const Slab& a, int sr, Slab& b, int dr, int
     const T* src = a.buf[buf] + k * a.plane + (long long)sr * S->pitch;
     T* dst = b.buf[buf] + k * b.plane + (long long)dr * S->pitch;
     cudaError_t e = cudaMemcpy2DAsync(dst, sizeof(T) * S->pitch, src, sizeof(T) * S->pitch,
-                                      sizeof(T) * S->nx, rows, cudaMemcpyDefault, b.stream);
+                                      sizeof(T) * S->nx, rows, cudaMemcpyDefault, b.bstream);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
-// Refreshes every slab's halo rows (buffer `buf`) from its neighbours' owned rows.
-cudaError_t exchange(le2d_slabs* S, int buf) {
+// Halo rows of buffer `buf` from the neighbours' band rows, after launch k: each copy on the
+// receiving slab's band stream, after the sending slab's band.
+cudaError_t exchange(le2d_slabs* S, int buf, long long k) {
   const int n = (int)S->s.size();
   for (int i = 0; i + 1 < n; ++i) {
     Slab& a = S->s[i];
     Slab& b = S->s[i + 1];
     // b's top halo <- a's last kHalo owned rows; a's bottom halo <- b's first kHalo owned rows
     cudaSetDevice(b.dev);
-    cudaError_t e = cudaStreamWaitEvent(b.stream, a.ev, 0);
+    cudaError_t e = cudaStreamWaitEvent(b.bstream, a.ev_band[k & 1], 0);
     if (e == cudaSuccess) e = copy_rows(S, a, a.h0 + (a.r1 - a.r0) - kHalo, b, 0, kHalo, buf);
     if (e != cudaSuccess) return e;
     cudaSetDevice(a.dev);
-    e = cudaStreamWaitEvent(a.stream, b.ev, 0);
+    e = cudaStreamWaitEvent(a.bstream, b.ev_band[k & 1], 0);
     if (e == cudaSuccess) e = copy_rows(S, b, b.h0, a, a.h0 + (a.r1 - a.r0), kHalo, buf);
     if (e != cudaSuccess) return e;
   }
@@ -118,7 +129,12 @@ void release(le2d_slabs* S) {
   for (Slab& sl : S->s) {
     cudaSetDevice(sl.dev);
     if (sl.stream) cudaStreamSynchronize(sl.stream);
-    if (sl.ev) cudaEventDestroy(sl.ev);
+    if (sl.bstream) cudaStreamSynchronize(sl.bstream);
+    for (int k = 0; k < 2; ++k) {
+      if (sl.ev_band[k]) cudaEventDestroy(sl.ev_band[k]);
+      if (sl.ev_int[k]) cudaEventDestroy(sl.ev_int[k]);
+    }
+    if (sl.bstream) cudaStreamDestroy(sl.bstream);
     if (sl.stream) cudaStreamDestroy(sl.stream);
     if (sl.mem) cudaFree(sl.mem);
     if (sl.d_status) cudaFree(sl.d_status);
@@ -130,6 +146,7 @@ int sync_all(le2d_slabs* S) {
   for (Slab& sl : S->s) {
     cudaSetDevice(sl.dev);
     cudaError_t e = cudaStreamSynchronize(sl.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sl.bstream);
     if (e != cudaSuccess) return S->fail(LE2D_ECUDA, "synchronize", e);
     int h = 0;
     e = cudaMemcpy(&h, sl.d_status, sizeof(int), cudaMemcpyDeviceToHost);
@@ -191,7 +208,13 @@ le2d_slabs* le2d_slabs_create(const le_task* task, int nslabs, const int* device
     if (e == cudaSuccess) e = cudaMalloc(&sl.mem, sizeof(T) * 2 * 5 * (size_t)sl.plane);
     if (e == cudaSuccess) e = cudaMalloc(&sl.d_status, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming);
+    int least = 0, greatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&sl.bstream, cudaStreamNonBlocking, greatest);
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+      e = cudaEventCreateWithFlags(&sl.ev_band[k], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.ev_int[k], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(sl.mem, 0, sizeof(T) * 2 * 5 * (size_t)sl.plane, sl.stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(sl.d_status, 0, sizeof(int), sl.stream);
     if (e != cudaSuccess) break;
@@ -301,34 +324,59 @@ int le2d_slabs_download(le2d_slabs* S, real* dst) {
   return rc;
 }
 
-// nsteps steps: launches of two steps (one at an odd end, and for SoA grids), each followed
-// by the halo exchange.  Asynchronous: le2d_slabs_download (or _wait) synchronises.
+// nsteps steps: launches of two steps (one at an odd end, and for SoA grids), each a band
+// and an interior launch per slab plus the halo copies.  Asynchronous: le2d_slabs_download
+// (or _wait) synchronises.
 int le2d_slabs_step_n(le2d_slabs* S, int nsteps) {
   if (!S || nsteps < 0) return LE2D_EINVAL;
   int prev = 0;
   cudaGetDevice(&prev);
   const int far_rot = S->stype == ST_SOA ? 1 : 0;
+  const int n = (int)S->s.size();
   int rc = LE2D_OK;
   for (int left = nsteps; left > 0 && rc == LE2D_OK;) {
     const bool two = !far_rot && left >= 2 && S->s[0].plan.depth == 2;
-    for (Slab& sl : S->s) {
+    const long long k = S->launches;
+    for (int i = 0; i < n && rc == LE2D_OK; ++i) {
+      Slab& sl = S->s[i];
       cudaSetDevice(sl.dev);
       const FusedPlan& pl = two ? sl.plan : sl.plan1;
       le2d::PairCtl pc;
       pc.status = sl.d_status;
       pc.wait_ns = kPairWaitNs;
-      cudaError_t e = le2d::launch_fused_step<T>(sl.buf[S->cur], sl.buf[S->cur ^ 1], S->nx, sl.nyl,
-                                                 S->pitch, sl.plane, S->c, far_rot, pl, pc, sl.stream);
-      if (e == cudaSuccess) e = cudaEventRecord(sl.ev, sl.stream);
-      if (e != cudaSuccess) {
-        rc = S->fail(LE2D_ECUDA, "step kernel launch", e);
-        break;
+      const int own0 = sl.h0, own1 = sl.h0 + (sl.r1 - sl.r0);
+      const int in0 = own0 + (i > 0 ? kHalo : 0), in1 = own1 - (i + 1 < n ? kHalo : 0);
+      const T* src = sl.buf[S->cur];
+      T* dst = sl.buf[S->cur ^ 1];
+      // interior rows, after this slab's previous band
+      cudaError_t e = cudaStreamWaitEvent(sl.stream, sl.ev_band[(k + 1) & 1], 0);
+      if (e == cudaSuccess)
+        e = le2d::launch_fused_rows<T>(src, dst, S->nx, sl.nyl, S->pitch, sl.plane, S->c, far_rot, pl, pc,
+                                       pl.seg_len, 1, &in0, &in1, sl.stream);
+      if (e == cudaSuccess) e = cudaEventRecord(sl.ev_int[k & 1], sl.stream);
+      // bands beside the cuts, after this slab's previous interior (and, on this stream, the
+      // halo copies into it)
+      int lo[2], hi[2], nr = 0;
+      if (i > 0) {
+        lo[nr] = own0;
+        hi[nr++] = own0 + kHalo;
       }
+      if (i + 1 < n) {
+        lo[nr] = own1 - kHalo;
+        hi[nr++] = own1;
+      }
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(sl.bstream, sl.ev_int[(k + 1) & 1], 0);
+      if (e == cudaSuccess && nr > 0)
+        e = le2d::launch_fused_rows<T>(src, dst, S->nx, sl.nyl, S->pitch, sl.plane, S->c, far_rot, pl, pc,
+                                       kHalo, nr, lo, hi, sl.bstream);
+      if (e == cudaSuccess) e = cudaEventRecord(sl.ev_band[k & 1], sl.bstream);
+      if (e != cudaSuccess) rc = S->fail(LE2D_ECUDA, "step kernel launch", e);
     }
     if (rc) break;
     S->cur ^= 1;
-    const cudaError_t e = exchange(S, S->cur);
+    const cudaError_t e = exchange(S, S->cur, k);
     if (e != cudaSuccess) rc = S->fail(LE2D_ECUDA, "halo exchange", e);
+    ++S->launches;
     left -= two ? 2 : 1;
   }
   cudaSetDevice(prev);

@@ -25,7 +25,21 @@ struct FusedParams {
   PairCtl pair;  // warp-pair waits
   // interior tiles: strips [s_lo, s_hi) x segments [g_lo, g_hi) (empty when lo >= hi)
   int s_lo, s_hi, g_lo, g_hi;
+  // rows the launch writes: segments [0, nseg0) cover rows [lo0, hi0), the rest [lo1, hi1)
+  int lo0, hi0, lo1, hi1, nseg0;
 };
+
+// Rows [y0, y1) of segment `seg` of the launch's row ranges.
+template <typename T>
+__device__ __forceinline__ void segment_rows(const FusedParams<T>& p, int seg, int& y0, int& y1) {
+  if (seg < p.nseg0) {
+    y0 = p.lo0 + seg * p.seg_len;
+    y1 = min(y0 + p.seg_len, p.hi0);
+  } else {
+    y0 = p.lo1 + (seg - p.nseg0) * p.seg_len;
+    y1 = min(y0 + p.seg_len, p.hi1);
+  }
+}
 
 // Tile of a task when the interior tiles come first (in segment-major order) and the
 // boundary tiles -- the segments above g_lo and from g_hi on, and the strips outside
@@ -79,8 +93,8 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) fused_step_kernel(const Fus
   int strip = task % p.nstrips;
   int seg = task / p.nstrips;
   if constexpr (F == 2) interior_first(p, task, strip, seg);
-  const int y0 = seg * p.seg_len;
-  const int y1 = min(y0 + p.seg_len, p.g.ny);
+  int y0, y1;
+  segment_rows(p, seg, y0, y1);
   if constexpr (D == 1 && F >= 1) {  // interior tiles on the lean loop
     const int xs = strip * strip_cols(V) - halo_lanes(V) * V;
     if (march::tile_is_interior1<T, V>(p.g, xs, y0, y1)) {
@@ -116,8 +130,8 @@ __global__ void __launch_bounds__(W * 32, MINB) fused_pair_kernel(const FusedPar
   int strip = task % p.nstrips;
   int seg = task / p.nstrips;
   if constexpr (F == 2) interior_first(p, task, strip, seg);
-  const int y0 = seg * p.seg_len;
-  const int y1 = min(y0 + p.seg_len, p.g.ny);
+  int y0, y1;
+  segment_rows(p, seg, y0, y1);
   T* smem = reinterpret_cast<T*>(base);
   unsigned u = 0;
   const march::RowTap<T> no_tap{nullptr, -1};
@@ -341,35 +355,62 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
 }
 
 template <typename T>
-cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pitch,
-                              long long plane, const StepConsts<T>& c, int far_rot,
-                              const FusedPlan& plan, const PairCtl& pair, cudaStream_t s) {
+cudaError_t launch_fused_rows(const T* src, T* dst, int nx, int ny, long long pitch, long long plane,
+                              const StepConsts<T>& c, int far_rot, const FusedPlan& plan,
+                              const PairCtl& pair, int seg_len, int nranges, const int* lo,
+                              const int* hi, cudaStream_t s) {
   if (plan.depth == 2 && far_rot) return cudaErrorInvalidValue;  // two steps assume clamped ends
   if (plan.warps_per_task == 2 && pair.status == nullptr) return cudaErrorInvalidValue;
+  if (nranges < 1 || nranges > 2 || seg_len < 1) return cudaErrorInvalidValue;
   FusedParams<T> p;
   p.pair = pair;
   p.g = march::GridRef<T>{src, dst, nx, ny, pitch, plane, far_rot};
   p.nstrips = plan.nstrips;
-  p.seg_len = plan.seg_len;
-  p.ntasks = plan.ntasks;
+  p.seg_len = seg_len;
+  p.lo0 = lo[0];
+  p.hi0 = hi[0];
+  p.lo1 = nranges == 2 ? lo[1] : 0;
+  p.hi1 = nranges == 2 ? hi[1] : 0;
+  for (int r = 0; r < nranges; ++r)
+    if (lo[r] < 0 || hi[r] > ny || lo[r] > hi[r]) return cudaErrorInvalidValue;
+  p.nseg0 = (p.hi0 - p.lo0 + seg_len - 1) / seg_len;
+  const int nseg1 = (p.hi1 - p.lo1 + seg_len - 1) / seg_len;
+  p.ntasks = plan.nstrips * (p.nseg0 + nseg1);
+  if (p.ntasks == 0) return cudaSuccess;
   p.c = c;
   p.yq = YPairs{};
   if constexpr (std::is_same<T, float>::value) p.yq = make_ypairs(c.y);
-  {  // the interior tiles' rectangle (tile_is_interior / tile_is_interior1: the strip inside
-     // [0, nx), the rows read, 2 per step beyond the tile's, inside [0, ny))
-    const int V = plan.lanes, L = plan.seg_len, margin = 2 * plan.depth;
+  {  // the interior tiles' rectangle, dealt out first (tile_is_interior / tile_is_interior1:
+     // the strip inside [0, nx), the rows read, 2 per step beyond the tile's, inside [0, ny));
+     // an ordering only -- every tile tests itself -- and empty for two ranges
+    const int V = plan.lanes, L = seg_len, margin = 2 * plan.depth;
     const int H = (plan.depth == 2 ? halo_lanes2(V) : halo_lanes(V)) * V;
     const int out = plan.depth == 2 ? strip_cols2(V) : strip_cols(V);
     p.s_lo = (H + out - 1) / out;
     p.s_hi = nx - 32 * V + H >= 0 ? (nx - 32 * V + H) / out + 1 : 0;
     if (p.s_hi > plan.nstrips) p.s_hi = plan.nstrips;
-    p.g_lo = (margin + L - 1) / L;
-    p.g_hi = ny >= margin ? (ny - margin) / L : 0;
-    if (p.s_hi < p.s_lo) p.s_hi = p.s_lo;
-    if (p.g_hi < p.g_lo) p.g_hi = p.g_lo;
+    const int base = p.lo0;
+    p.g_lo = margin > base ? (margin - base + L - 1) / L : 0;
+    p.g_hi = ny - margin - base >= 0 ? (ny - margin - base) / L : 0;
+    if (p.g_hi > p.nseg0) p.g_hi = p.nseg0;
+    if (p.s_hi < p.s_lo || nranges == 2) p.s_hi = p.s_lo;
+    if (p.g_hi < p.g_lo || nranges == 2) p.g_hi = p.g_lo;
   }
-  with_variant<T, LaunchOp, int>(plan.variant, plan, p, s);
+  FusedPlan pl = plan;
+  pl.ntasks = p.ntasks;
+  const int tasks_per_block = plan.threads / 32 / plan.warps_per_task;
+  pl.blocks = (p.ntasks + tasks_per_block - 1) / tasks_per_block;
+  with_variant<T, LaunchOp, int>(plan.variant, pl, p, s);
   return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pitch,
+                              long long plane, const StepConsts<T>& c, int far_rot,
+                              const FusedPlan& plan, const PairCtl& pair, cudaStream_t s) {
+  const int lo = 0, hi = ny;
+  return launch_fused_rows<T>(src, dst, nx, ny, pitch, plane, c, far_rot, plan, pair, plan.seg_len, 1,
+                              &lo, &hi, s);
 }
 
 #define LE2D_INST(T)                                                                            \
@@ -380,7 +421,11 @@ cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pi
   template FusedPlan plan_fused<T>(int, int, int, int, int);                                    \
   template cudaError_t launch_fused_step<T>(const T*, T*, int, int, long long, long long,       \
                                             const StepConsts<T>&, int, const FusedPlan&,        \
-                                            const PairCtl&, cudaStream_t);
+                                            const PairCtl&, cudaStream_t);                      \
+  template cudaError_t launch_fused_rows<T>(const T*, T*, int, int, long long, long long,       \
+                                            const StepConsts<T>&, int, const FusedPlan&,        \
+                                            const PairCtl&, int, int, const int*, const int*,   \
+                                            cudaStream_t);
 LE2D_INST(float)
 LE2D_INST(double)
 #undef LE2D_INST

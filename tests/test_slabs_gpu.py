@@ -69,3 +69,54 @@ def test_slabs_reject_thin_slabs():
             capi.Slabs(lib, t, [0, 0, 0, 0])  # 30 rows: fewer than 8 per slab
     finally:
         lib.le_free_task(t)
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
+def test_rank_slabs_exchange_rows_on_device(prec):
+    """The one-process-per-rank decomposition (le2d_b200.dist_slabs) with its ranks'
+    slabs as tasks on this one GPU: the 4 owned rows beside each cut leave through
+    le2d_rows_out into the ranks' CUDA send buffers and come back through le2d_rows_in
+    from their receive buffers as the neighbour's halo rows (copied here buffer to buffer
+    where NCCL send/recv carries them between processes); the gathered owned rows equal
+    the whole grid stepped by one task, bit for bit."""
+    torch = pytest.importorskip("torch")
+    from le2d_b200.dist_slabs import SlabExchange, local_rows
+
+    lib = capi.Lib(prec)
+    c = dict(nx=300, ny=90, hx=1.0, hy=0.9, c1=2.3, c2=1.2, rho=1.6, dt=0.17, stype=ST_AOS)
+    rng = np.random.default_rng(3)
+    g0 = rng.uniform(-1, 1, 5 * c["nx"] * c["ny"]).astype(lib.dtype)
+    steps, world = 9, 3
+    want = _whole(lib, c, g0, steps)
+    dtype = torch.float32 if prec == "f" else torch.float64
+    stream = torch.cuda.current_stream().cuda_stream
+    ranks = []
+    for r in range(world):
+        x = SlabExchange(None, r, world, c["nx"], c["ny"], lambda s: torch.empty(s, dtype=dtype, device="cuda"))
+        mat = lib.le_init_material(c["c1"], c["c2"], c["rho"])
+        t = lib.le_init_task(c["dt"], (c["hx"], c["hy"]), mat, (c["nx"], x.nyl), ST_AOS)
+        assert lib.upload(t, local_rows(g0, c["nx"], c["ny"], ST_AOS, x.r0 - x.h0, x.r1 + x.h1)) == 0
+        ranks.append((x, t))
+    try:
+        left = steps
+        while left > 0:
+            k = min(2, left)
+            for x, t in ranks:
+                assert lib.step_n(t, k) == 0
+            for (a, ta), (b, tb) in zip(ranks, ranks[1:]):  # each cut, both directions
+                assert lib.rows_out(ta, a.h0 + a.own - a.halo, a.halo, a.down[0].data_ptr(), stream) == 0
+                assert lib.rows_out(tb, b.h0, b.halo, b.up[0].data_ptr(), stream) == 0
+                b.up[1].copy_(a.down[0])
+                a.down[1].copy_(b.up[0])
+                assert lib.rows_in(tb, 0, b.halo, b.up[1].data_ptr(), stream) == 0
+                assert lib.rows_in(ta, a.h0 + a.own, a.halo, a.down[1].data_ptr(), stream) == 0
+            left -= k
+        parts = []
+        for x, t in ranks:
+            g = np.zeros(5 * c["nx"] * x.nyl, lib.dtype)
+            assert lib.download(t, g) == 0 and lib.last_error(t) == 0
+            parts.append(local_rows(g, c["nx"], x.nyl, ST_AOS, x.h0, x.h0 + x.own))
+        assert np.concatenate(parts).tobytes() == want.tobytes()
+    finally:
+        for x, t in ranks:
+            lib.le_free_task(t)
