@@ -110,7 +110,9 @@ __device__ __forceinline__ float ratio(float a, float b) {
 // 0 and 2: the select returns copysign(inf, a), which the limiter maps the same way (a is
 // never -0 either).  Outside the supported range: magnitudes of 2^1022 and above (state
 // values near overflow) and operands below about 2^-970, where the residual underflows.
-// A select, not a branch: a branch per ratio costs more than the division.
+// A select, not a branch: a branch per ratio costs more than the division.  The tie test
+// reads b's high word with an integer compare (zero for +0 and for nothing else in range),
+// which keeps it off the FP64 pipe the step is bound by.
 __device__ __forceinline__ double ratio(double a, double b) {
   double y0;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(b));
@@ -118,7 +120,7 @@ __device__ __forceinline__ double ratio(double a, double b) {
   const double q = a * y;
   const double r = fma(fma(-b, q, a), y, q);
   const double inf = __hiloint2double((__double2hiint(a) & (int)0x80000000) | 0x7ff00000, 0);
-  return b == 0.0 ? inf : r;
+  return __double2hiint(b) == 0 ? inf : r;
 }
 
 __device__ __forceinline__ float max3(float a, float b, float c) {
