@@ -108,11 +108,12 @@ long long row_pitch(int nx) { return le2d::row_pitch_elems(nx); }
 // measured on large grids (FP32: two steps per launch on producer / consumer warp pairs,
 // 4 columns per lane, 16 warps per SM, one pair per block, interior tiles first and on the
 // lean loops; FP64: one step per launch, 2 columns per lane, interior tiles first and on
-// the lean one-step loop, 12 warps per SM -- the FP64 two-step variants measured slower).
+// the lean one-step loop in 128 registers, 16 warps per SM -- the FP64 two-step variants
+// measured slower).
 int default_variant() {
   static int v = -2;
   if (v == -2) {
-    const int dflt = sizeof(T) == 4 ? 13 : 14;
+    const int dflt = sizeof(T) == 4 ? 13 : 15;
     const char* e = getenv("LE2D_FUSED_VARIANT");
     v = e ? atoi(e) : dflt;
     if (v < 0 || v >= le2d::fused_variant_count<T>()) v = dflt;
@@ -136,7 +137,7 @@ void replan(DevTask* d, int variant, int seg_len) {
   d->plan = p;
   d->plan1 = p;
   if (p.depth != 1) {  // odd remainders and le_step_soa run single steps
-    const int v = sizeof(T) == 4 ? 2 : 14;  // the fastest one-step variant
+    const int v = sizeof(T) == 4 ? 2 : 15;  // the fastest one-step variant
     d->plan1 = le2d::plan_fused<T>(d->nx, d->ny, v, le2d::fused_resident_warps<T>(dev, v), kMinSeg);
   }
   if (d->graph) cudaGraphExecDestroy(d->graph);

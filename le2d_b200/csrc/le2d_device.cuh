@@ -141,7 +141,7 @@ __device__ __forceinline__ float psi(float r, float kc) {
 // one follows from r's high word h alone, because the breakpoints 0.5, 1 and 2 have zero low
 // words (so, for r >= 0, r < 1 <=> h < h(1), and so on): r in [1, 2) keeps r, below that 1,
 // from 2 on (with +inf) 2 -- a clamp of h to [h(1), h(2)] with the low word kept only
-// inside -- then 2r below 0.5 and 0 for negative r.  The FP64 ratio never returns NaN (a tie
+// inside -- then 2r below 0.5 and 0 for r <= 0.  The FP64 ratio never returns NaN (a tie
 // gives copysign(inf, a), see ratio(double)); a positive NaN would land on 2 like the
 // reference's superbee(NaN).  The product kc * superbee(r), kc = (1 - k) / 2, rounds like
 // the reference's `limiter(r) / 2.0 * (1.0 - c)`: halving is exact.  The reference returns
@@ -149,13 +149,15 @@ __device__ __forceinline__ float psi(float r, float kc) {
 __device__ __forceinline__ double psi(double r, double kc) {
   constexpr int kH05 = 0x3fe00000, kH1 = 0x3ff00000, kH2 = 0x40000000;  // high words of 0.5, 1, 2
   const int h = __double2hiint(r), l = __double2loint(r);
-  const double r2 = r + r;
-  const bool small = h < kH05, neg = h < 0;
+  const bool small = h < kH05, pos = h > 0;
   // written as selects: a branch here would diverge within the warp
   int ho = min(max(h, kH1), kH2);
   int lo = h >= kH1 && h < kH2 ? l : 0;
-  ho = small ? (neg ? 0 : __double2hiint(r2)) : ho;  // 0 <= r < 0.5: 2r; r < 0: 0
-  lo = small ? (neg ? 0 : __double2loint(r2)) : lo;
+  // 0 < r < 0.5: 2r, by one more in the exponent field (r is a normal number there: the
+  // ratios' operands are at least 2^-73 or 0); r <= 0: 0.  An integer add instead of a
+  // floating-point one keeps the FP64 pipe, which bounds the step, free.
+  ho = small ? (pos ? h + 0x00100000 : 0) : ho;
+  lo = small ? (pos ? l : 0) : lo;
   return kc * __hiloint2double(ho, lo);
 }
 

@@ -65,9 +65,9 @@ struct Slab {
 };
 
 // Variant of each launch: FP32 two steps on warp pairs (one-step variant 2 for odd
-// remainders and SoA), FP64 one step (variant 14), as for whole tasks.
-int two_step_variant() { return sizeof(T) == 4 ? 13 : 14; }
-int one_step_variant() { return sizeof(T) == 4 ? 2 : 14; }
+// remainders and SoA), FP64 one step (variant 15), as for whole tasks.
+int two_step_variant() { return sizeof(T) == 4 ? 13 : 15; }
+int one_step_variant() { return sizeof(T) == 4 ? 2 : 15; }
 
 }  // namespace
 
