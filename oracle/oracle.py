@@ -171,6 +171,28 @@ class ReferencePthread:
         return t
 
 
+class ReferenceTiling:
+    """The reference's two-buffer schedule tiling/ le_step_all2 (oracle/_ref), one precision:
+    zero ring of two nodes around the grid, increments associated (v + d1) + d2."""
+
+    def __init__(self, prec: str):
+        path = os.path.join(REF_DIR, f"libref_tiling_{prec}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.dtype = np_dtype(prec)
+        L = self.lib = ctypes.CDLL(path)
+        R = _real(prec)
+        L.ref_tiling_run.argtypes = [_I, _I, R, R, R, R, R, R, _P, _I]
+        assert L.ref_tiling_real_size() == (4 if prec == "f" else 8)
+
+    @staticmethod
+    def available(prec: str = "d") -> bool:
+        return os.path.exists(os.path.join(REF_DIR, f"libref_tiling_{prec}.so"))
+
+    def run(self, grid, nx, ny, dt, hx, hy, c1, c2, rho, steps):
+        assert self.lib.ref_tiling_run(nx, ny, dt, hx, hy, c1, c2, rho, _ptr(grid), steps) == 0
+
+
 def aos_to_soa(g: np.ndarray, nx: int, ny: int) -> np.ndarray:
     return np.ascontiguousarray(g.reshape(ny, nx, 5).transpose(2, 0, 1)).reshape(-1)
 

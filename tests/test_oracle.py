@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from golden_cases import arrays, cases, summary
-from oracle.oracle import ST_AOS, ST_SOA, Oracle, Reference, aos_to_soa, fields, rel_l2
+from oracle.oracle import ST_AOS, ST_SOA, Oracle, Reference, ReferenceTiling, aos_to_soa, fields, rel_l2
 
 PRECS = ("f", "d")
 
@@ -127,3 +127,29 @@ def test_live_reference_random_cases(prec):
         ref.run(g0, nx, ny, dt, hx, hy, c1, c2, rho, stype, steps, threads=2)
         o.run(g1, nx, ny, dt, hx, hy, c1, c2, rho, stype, steps)
         assert g0.tobytes() == g1.tobytes()
+
+
+@pytest.mark.skipif(not ReferenceTiling.available("d"), reason="oracle/_ref not built")
+@pytest.mark.parametrize("prec", PRECS)
+def test_tiling_schedule_matches_away_from_the_edges(prec):
+    """The reference's two-buffer schedule (tiling/ le_step_all2: zero ring of two nodes
+    around the grid, increments associated (v + d1) + d2) against the restatement of simple/
+    on the nodes its ends cannot reach after s steps (2 per step from each edge): the same
+    scheme with other roundings -- FP64 within 1e-12, FP32 within 1e-5 relative L2."""
+    o, t = Oracle(prec), ReferenceTiling(prec)
+    nx, ny, steps = 96, 80, 6
+    rng = np.random.default_rng(11)
+    g = np.zeros(5 * nx * ny, o.dtype)
+    for _ in range(3):
+        o.set_ball(g, nx, ny, 1.0, 0.9, ST_AOS, float(rng.uniform(20, 76)), float(rng.uniform(20, 60)),
+                   float(rng.uniform(5, 15)), float(rng.uniform(-2, 2)))
+    g[0::5] += rng.uniform(-1e-3, 1e-3, nx * ny).astype(o.dtype)
+    a, b = g.copy(), g.copy()
+    o.run(a, nx, ny, 0.17, 1.0, 0.9, 2.3, 1.2, 1.6, ST_AOS, steps)
+    t.run(b, nx, ny, 0.17, 1.0, 0.9, 2.3, 1.2, 1.6, steps)
+    m = 2 * steps
+    fa = fields(a, nx, ny, ST_AOS)[:, m:ny - m, m:nx - m]
+    fb = fields(b, nx, ny, ST_AOS)[:, m:ny - m, m:nx - m]
+    err = rel_l2(fa, fb)
+    assert np.all(err <= (1e-12 if prec == "d" else 1e-5)), err
+    assert not np.array_equal(a, b)  # the ends differ (zero ring against clamped)

@@ -381,6 +381,48 @@ def test_exact_ties(libs, prec, mat):
 
 
 @pytest.mark.parametrize("prec", ["f", "d"])
+def test_temporal_blocking_against_tiling_schedule(libs, prec):
+    """The two-step (temporal-blocking) variants against the reference's own alternative
+    schedule, tiling/ le_step_all2 (two buffers, a zero ring of two nodes around the grid,
+    increments associated (v + d1) + d2), run from its sources (oracle/_ref): on the nodes
+    that schedule's ends cannot reach after s steps (2 per step from each edge) the two are
+    the same scheme with other roundings -- FP64 within 1e-12, FP32 within 1e-5."""
+    from oracle.oracle import ReferenceTiling
+
+    if not ReferenceTiling.available(prec):
+        pytest.skip("oracle/_ref not built")
+    lib = libs[prec]
+    nx, ny, steps = 300, 190, 6
+    c = dict(nx=nx, ny=ny, hx=1.0, hy=0.9, c1=2.3, c2=1.2, rho=1.6, dt=0.17, stype=ST_AOS)
+    rng = np.random.default_rng(12)
+    o = Oracle(prec)
+    g0 = np.zeros(5 * nx * ny, o.dtype)
+    for _ in range(4):
+        o.set_ball(g0, nx, ny, 1.0, 0.9, ST_AOS, float(rng.uniform(30, 270)), float(rng.uniform(30, 140)),
+                   float(rng.uniform(5, 25)), float(rng.uniform(-2, 2)))
+    g0[0::5] += rng.uniform(-1e-3, 1e-3, nx * ny).astype(o.dtype)
+    want = g0.copy()
+    ReferenceTiling(prec).run(want, nx, ny, c["dt"], c["hx"], c["hy"], c["c1"], c["c2"], c["rho"], steps)
+    m = 2 * steps
+    fw = fields(want, nx, ny, ST_AOS)[:, m:ny - m, m:nx - m]
+    two_step = [v for v, depth in sorted(variants(lib).items()) if depth == 2]
+    assert two_step
+    for var in two_step:
+        t = make_task(lib, c)
+        try:
+            assert lib.set_variant(t, var, 0) == 0
+            assert lib.upload(t, g0.copy()) == 0
+            assert lib.step_n(t, steps) == 0
+            got = np.zeros_like(g0)
+            assert lib.download(t, got) == 0 and lib.last_error(t) == 0
+        finally:
+            lib.le_free_task(t)
+        err = rel_l2(fields(got, nx, ny, ST_AOS)[:, m:ny - m, m:nx - m], fw)
+        print(f"\ntiling/{prec}/v{var}: interior rel_l2={np.array2string(err, precision=2)}")
+        assert np.all(err <= TOL[prec]), (var, err)
+
+
+@pytest.mark.parametrize("prec", ["f", "d"])
 def test_uniform_state_is_fixed_point(libs, prec):
     c = dict(nx=257, ny=131, hx=1.0, hy=1.0, c1=2.0, c2=1.0, rho=1.0, dt=0.25, stype=ST_AOS)
     g0 = np.tile(np.array([0.3, -0.2, 1.5, 0.25, -0.7], libs[prec].dtype), 257 * 131)

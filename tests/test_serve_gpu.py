@@ -132,3 +132,39 @@ def test_failed_solve_fails_alone(lib, monkeypatch):
             assert srv.result(t).tobytes() == want.tobytes()
         s = srv.stats()
         assert s["failed"] == 1 and s["completed"] == len(others)
+
+
+def test_abandoned_requests_and_shutdown_mid_flight(lib):
+    """A client that dies after submitting (its thread exits without waiting or releasing):
+    its requests still complete without holding up anyone else's, and their tickets stay
+    pollable.  A server destroyed while requests are queued and running returns promptly
+    and gives its device memory back: a server with the same budget runs afterwards."""
+    probs = small_set(35, 4, 40, 200, 20, 60)
+    budget = 1 << 29
+    with capi.Server(lib, budget, window_steps=8) as srv:
+        abandoned = []
+        dead = threading.Thread(target=lambda: abandoned.extend(
+            srv.submit(srv_problem(lib, p), disks=p.disks) for p in probs[:3]))
+        dead.start()
+        dead.join()  # the client is gone
+        t = srv.submit(srv_problem(lib, probs[3]), disks=probs[3].disks)
+        assert srv.wait(t, 60.0) == 0
+        want, _ = solve_alone(lib, probs[3], ST_AOS)
+        assert srv.result(t).tobytes() == want.tobytes()
+        deadline = time.time() + 60
+        while any(srv.poll(a) == 0 for a in abandoned) and time.time() < deadline:
+            time.sleep(0.01)
+        assert [srv.poll(a) for a in abandoned] == [1, 1, 1]
+        assert srv.stats()["completed"] == 4
+    big = workloads.Problem(2048, 2048, 1, 1, 2, 1, 1, 0.25, 4000, [(1024.0, 1024.0, 100.0, 1.0)])
+    srv = capi.Server(lib, budget, window_steps=64)
+    ts = [srv.submit(srv_problem(lib, big), disks=big.disks) for _ in range(5)]
+    assert all(x > 0 for x in ts)
+    time.sleep(0.2)  # some admitted and running, others queued
+    t0 = time.time()
+    srv.close()
+    assert time.time() - t0 < 30.0
+    with capi.Server(lib, budget, window_steps=8) as srv2:
+        t = srv2.submit(srv_problem(lib, probs[0]), disks=probs[0].disks)
+        assert srv2.wait(t, 60.0) == 0
+        assert srv2.stats()["arena_capacity"] >= budget * 0.99
