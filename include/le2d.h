@@ -231,6 +231,13 @@ double le2d_now(void);
 int le2d_rows_out(le_task *task, int row0, int nrows, real *dev_buf, void *stream);
 int le2d_rows_in(le_task *task, int row0, int nrows, const real *dev_buf, void *stream);
 
+/* Bounds-checked build (the library under le2d_b200/lib/checked/, compiled with LE2D_CHECK):
+ * every access of the state by the step kernels checks that it stays inside the buffer it
+ * addresses and is skipped and counted when it does not.  Returns 1 in the checked build
+ * (*count = accesses refused on the current device since the last call), 0 in the normal
+ * build (*count = 0).  A stand-in for a memory checker on machines where none can run. */
+int le2d_check_violations(unsigned long long *count);
+
 /* Layout of the device state (SoA, 5 planes of n.y rows with a padded row pitch). */
 int le2d_device_layout(const le_task *task, long long *pitch_elems, long long *plane_elems);
 

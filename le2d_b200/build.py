@@ -3,7 +3,9 @@
     python -m le2d_b200.build            # both precisions
     python -m le2d_b200.build --verbose  # also print ptxas register / spill reports
 
-Objects go to le2d_b200/_build/, libraries to le2d_b200/lib/.  The host compiler
+Objects go to le2d_b200/_build/, libraries to le2d_b200/lib/, and the bounds-checked build
+(LE2D_CHECK: every state access of the step kernels checked and counted, for tests) to
+le2d_b200/lib/checked/.  The host compiler
 runs with -ffp-contract=off so the host-side material and initial-condition
 arithmetic rounds like the reference build (x86-64 baseline, no FMA).
 """
@@ -38,8 +40,10 @@ def nvcc() -> str:
 def _flags(prec: str) -> list[str]:
     f = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
                 "-I", INCLUDE, "-I", CSRC]
-    if prec == "d":
+    if prec.startswith("d"):
         f += ["-DUSE_DOUBLE"]
+    if prec.endswith("_check"):
+        f += ["-DLE2D_CHECK"]
     return f
 
 
@@ -73,14 +77,21 @@ def _compile(prec: str, src: str, verbose: bool) -> str:
     return obj
 
 
-def build(verbose: bool = False, precs=("f", "d")) -> list[str]:
+def build(verbose: bool = False, precs=("f", "d"), checked: bool = True) -> list[str]:
+    """The libraries of each precision; with `checked` also the bounds-checked build
+    (LE2D_CHECK) under lib/checked/."""
     os.makedirs(LIBDIR, exist_ok=True)
+    variants = list(precs) + ([p + "_check" for p in precs] if checked else [])
     out = []
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 2)) as ex:
-        futs = {(p, s): ex.submit(_compile, p, s, verbose) for p in precs for s in SOURCES}
+        futs = {(p, s): ex.submit(_compile, p, s, verbose) for p in variants for s in SOURCES}
         objs = {k: f.result() for k, f in futs.items()}
-    for p in precs:
-        lib = os.path.join(LIBDIR, f"lible2d_{p}.so")
+    for p in variants:
+        if p.endswith("_check"):
+            os.makedirs(os.path.join(LIBDIR, "checked"), exist_ok=True)
+            lib = os.path.join(LIBDIR, "checked", f"lible2d_{p[:-6]}.so")
+        else:
+            lib = os.path.join(LIBDIR, f"lible2d_{p}.so")
         pobjs = [objs[(p, s)] for s in SOURCES]
         if _newer(lib, pobjs):
             cmd = [nvcc(), "-shared", "-o", lib] + pobjs + ARCH + ["-Xlinker", "-z,defs"]

@@ -49,7 +49,7 @@ EXPORTS = [
     "le2d_batch_autotune", "le2d_batch_autotune_reset",
     "le2d_slabs_create", "le2d_slabs_destroy", "le2d_slabs_rows", "le2d_slabs_upload",
     "le2d_slabs_download", "le2d_slabs_step_n", "le2d_slabs_wait", "le2d_selftest_ratio",
-    "le2d_rows_out", "le2d_rows_in",
+    "le2d_rows_out", "le2d_rows_in", "le2d_check_violations",
 ]
 
 LE2D_DIAG_NOALLOC_MAX_ROWS = 16384
@@ -70,8 +70,8 @@ class LibraryMissing(RuntimeError):
     pass
 
 
-def lib_path(prec: str) -> str:
-    return os.path.join(LIBDIR, f"lible2d_{prec}.so")
+def lib_path(prec: str, checked: bool = False) -> str:
+    return os.path.join(LIBDIR, "checked" if checked else "", f"lible2d_{prec}.so")
 
 
 def _types(prec: str):
@@ -105,8 +105,8 @@ def _types(prec: str):
 class Lib:
     """One precision of the library ('f' or 'd')."""
 
-    def __init__(self, prec: str = "f"):
-        path = lib_path(prec)
+    def __init__(self, prec: str = "f", checked: bool = False):
+        path = lib_path(prec, checked)
         if not os.path.exists(path):
             raise LibraryMissing(f"{path} is not built (python -m le2d_b200.build)")
         self.prec = prec
@@ -193,6 +193,7 @@ class Lib:
         L.le2d_slabs_download.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.le2d_slabs_step_n.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.le2d_slabs_wait.argtypes = [ctypes.c_void_p]
+        L.le2d_check_violations.argtypes = [P(ctypes.c_ulonglong)]
         L.le2d_rows_out.argtypes = [P(self.le_task), ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.le2d_rows_in.argtypes = [P(self.le_task), ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.le2d_selftest_ratio.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
@@ -332,6 +333,12 @@ class Lib:
         rc = self.lib.le2d_diagnostics_noalloc(d_state, nx, ny, pitch, plane, hx, hy, c1, c2, rho,
                                                stream or None, ctypes.byref(d))
         return rc, {"energy": d.energy, "sumsq": list(d.sumsq), "maxabs": list(d.maxabs)}
+
+    def check_violations(self):
+        """(is_checked_build, state accesses refused since the last call)."""
+        n = ctypes.c_ulonglong(0)
+        checked = self.lib.le2d_check_violations(ctypes.byref(n))
+        return bool(checked), n.value
 
     def rows_out(self, t, row0: int, nrows: int, dev_ptr: int, stream: int = 0) -> int:
         """Rows of the task's state into a device buffer [5][nrows][nx] (e.g. a CUDA tensor)."""

@@ -309,6 +309,18 @@ cudaError_t launch_batch(const BatchInst<T>* insts, const BatchTile* tiles,
   return cudaGetLastError();
 }
 
+#ifdef LE2D_CHECK
+unsigned long long check_violations_batch() {
+  unsigned long long v = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&v, march::g_check_violations, sizeof(v)) != cudaSuccess ||
+      cudaMemcpyToSymbol(march::g_check_violations, &zero, sizeof(zero)) != cudaSuccess) {
+    cudaGetLastError();
+    return ~0ULL;  // unreadable: reported as violations
+  }
+  return v;
+}
+#endif
+
 #define LE2D_INST(T)                                                                            \
   template int batch_lanes<T>();                                                                \
   template int batch_depth<T>();                                                                \

@@ -943,6 +943,17 @@ int copy_rows(le_task* task, int row0, int nrows, T* dev_buf, void* stream, bool
 
 extern "C" {
 
+int le2d_check_violations(unsigned long long* count) {
+#ifdef LE2D_CHECK
+  const unsigned long long a = le2d::check_violations_fused(), b = le2d::check_violations_batch();
+  if (count) *count = a == ~0ULL || b == ~0ULL ? ~0ULL : a + b;
+  return 1;
+#else
+  if (count) *count = 0;
+  return 0;
+#endif
+}
+
 int le2d_rows_out(le_task* task, int row0, int nrows, real* dev_buf, void* stream) {
   return copy_rows(task, row0, nrows, dev_buf, stream, true);
 }

@@ -69,6 +69,13 @@ cudaError_t launch_fused_rows(const T* src, T* dst, int nx, int ny, long long pi
                               const PairCtl& pair, int seg_len, int nranges, const int* lo,
                               const int* hi, cudaStream_t s);
 
+#ifdef LE2D_CHECK
+// Bounds-checked build: accesses of the state the step kernels refused (outside the buffer),
+// on the current device, since the last call, per translation unit.
+unsigned long long check_violations_fused();
+unsigned long long check_violations_batch();
+#endif
+
 // The plain scheme: one sweep (axis 0 = x, 1 = y) src -> dst, one thread per node, the
 // reference's tvd2 formula node by node (two divisions per invariant).
 template <typename T>

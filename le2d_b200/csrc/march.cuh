@@ -60,6 +60,63 @@ struct GridRef {
   int far_rot;
 };
 
+// Bounds-checked build (-DLE2D_CHECK, the library under lib/checked/): every access of the
+// state checks that it stays inside the five planes of the buffer it addresses -- row in
+// [0, ny), columns in [0, pitch) -- and counts it in g_check_violations and skips it (a load
+// reads 0) when it does not, so a wrong index is reported without touching memory outside
+// the buffer.  In the normal build the checks are constant true and vanish.  Each
+// translation unit that marches tiles has its own counter; check_violations() in that unit
+// reads and clears it.
+#ifdef LE2D_CHECK
+static __device__ unsigned long long g_check_violations = 0;
+#endif
+
+template <typename T>
+__device__ __forceinline__ bool in_grid(const T* base, const T* p, long long pitch, long long plane,
+                                        int ny, int ncols) {
+#ifdef LE2D_CHECK
+  const long long off = p - base;
+  bool ok = off >= 0 && off < 5 * plane;
+  if (ok) {
+    const long long q = off % plane;
+    ok = q / pitch < ny && q % pitch + ncols <= pitch;
+  }
+  if (!ok) atomicAdd(&g_check_violations, 1ULL);
+  return ok;
+#else
+  return true;
+#endif
+}
+template <typename T>
+__device__ __forceinline__ bool in_src_checked(const GridRef<T>& g, const T* p, int ncols) {
+  return in_grid(g.src, p, g.pitch, g.plane, g.ny, ncols);
+}
+template <typename T>
+__device__ __forceinline__ bool in_dst_checked(const GridRef<T>& g, const T* p, int ncols) {
+  return in_grid<T>(g.dst, p, g.pitch, g.plane, g.ny, ncols);
+}
+// A receiver line: two rows (vx, vy) of `pitch` elements per sample.
+__device__ __forceinline__ bool in_line_checked(int col0, int ncols, long long pitch) {
+#ifdef LE2D_CHECK
+  const bool ok = col0 >= 0 && col0 + ncols <= pitch;
+  if (!ok) atomicAdd(&g_check_violations, 1ULL);
+  return ok;
+#else
+  return true;
+#endif
+}
+// The checks as they appear at the accesses: the literal `true` in the normal build, so its
+// code is exactly the unchecked code.
+#ifdef LE2D_CHECK
+#define in_src(g, p, n) in_src_checked(g, p, n)
+#define in_dst(g, p, n) in_dst_checked(g, p, n)
+#define in_line(c, n, pitch) in_line_checked(c, n, pitch)
+#else
+#define in_src(g, p, n) true
+#define in_dst(g, p, n) true
+#define in_line(c, n, pitch) true
+#endif
+
 // Optional receiver line: when `row` >= 0 and the march writes that row, vx and vy of
 // the written columns also go to out[0 * pitch + i] and out[1 * pitch + i].
 template <typename T>
@@ -83,14 +140,19 @@ __device__ __forceinline__ void load_row(T (&f)[NF][V], const GridRef<T>& g, int
   const T* base = g.src + (long long)row * g.pitch;
   if (interior) {
 #pragma unroll
-    for (int k = 0; k < NF; ++k)
-      unpack(load_state<COHERENT>(reinterpret_cast<const VT*>(base + k * g.plane + col0)), f[k]);
+    for (int k = 0; k < NF; ++k) {
+      const T* p = base + k * g.plane + col0;
+      unpack(in_src(g, p, V) ? load_state<COHERENT>(reinterpret_cast<const VT*>(p)) : VT{}, f[k]);
+    }
   } else {
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const int cc = min(max(col0 + v, 0), g.nx - 1);
 #pragma unroll
-      for (int k = 0; k < NF; ++k) f[k][v] = load_state<COHERENT>(base + k * g.plane + cc);
+      for (int k = 0; k < NF; ++k) {
+        const T* p = base + k * g.plane + cc;
+        f[k][v] = in_src(g, p, 1) ? load_state<COHERENT>(p) : T(0);
+      }
     }
   }
 }
@@ -296,13 +358,19 @@ __device__ __forceinline__ void fetch_row(T* slot, const GridRef<T>& g, int row,
   const T* base = g.src + (long long)row * g.pitch;
   if (interior) {
 #pragma unroll
-    for (int k = 0; k < NF; ++k) cp_async<V * (int)sizeof(T)>(slot + k * kIn, base + k * g.plane + col0);
+    for (int k = 0; k < NF; ++k) {
+      const T* p = base + k * g.plane + col0;
+      if (in_src(g, p, V)) cp_async<V * (int)sizeof(T)>(slot + k * kIn, p);
+    }
   } else {
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       const int cc = min(max(col0 + v, 0), g.nx - 1);
 #pragma unroll
-      for (int k = 0; k < NF; ++k) slot[k * kIn + v] = load_state<COHERENT>(base + k * g.plane + cc);
+      for (int k = 0; k < NF; ++k) {
+        const T* p = base + k * g.plane + cc;
+        slot[k * kIn + v] = in_src(g, p, 1) ? load_state<COHERENT>(p) : T(0);
+      }
     }
   }
   cp_async_commit();
@@ -584,8 +652,9 @@ __device__ __forceinline__ void march_tile(const GridRef<T>& g, const StepConsts
       yp.apply(gf, cy);
       T* out = g.dst + (long long)row * g.pitch + col0;
 #pragma unroll
-      for (int k = 0; k < NF; ++k) store_if(writer, reinterpret_cast<VT*>(out + k * g.plane), pack(gf[k]));
-      if (TAP && row == tap.row && writer) {
+      for (int k = 0; k < NF; ++k)
+        store_if(writer && in_dst(g, out + k * g.plane, V), reinterpret_cast<VT*>(out + k * g.plane), pack(gf[k]));
+      if (TAP && row == tap.row && writer && in_line(col0, V, g.pitch)) {
         *reinterpret_cast<VT*>(tap.out + col0) = pack(gf[VX]);
         *reinterpret_cast<VT*>(tap.out + g.pitch + col0) = pack(gf[VY]);
       }

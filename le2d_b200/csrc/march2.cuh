@@ -172,7 +172,8 @@ __device__ __forceinline__ void march_tile2(const GridRef<T>& g, const StepConst
           if (writer) {
             T* out = g.dst + (long long)(bin - 2) * g.pitch + col0;
 #pragma unroll
-            for (int k = 0; k < NF; ++k) *reinterpret_cast<VT*>(out + k * g.plane) = pack(gb[k]);
+            for (int k = 0; k < NF; ++k)
+              if (in_dst(g, out + k * g.plane, V)) *reinterpret_cast<VT*>(out + k * g.plane) = pack(gb[k]);
           }
         }
         yb.right(c.y);

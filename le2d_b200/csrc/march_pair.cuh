@@ -129,6 +129,7 @@ template <typename T, int V>
 __device__ __forceinline__ void tap_row(const RowTap<T>& tap, long long pitch, int col0,
                                         const T (&f)[NF][V]) {
   using VT = typename Vec<T, V>::type;
+  if (!in_line(col0, V, pitch)) return;
   *reinterpret_cast<VT*>(tap.out + col0) = pack(f[VX]);
   *reinterpret_cast<VT*>(tap.out + pitch + col0) = pack(f[VY]);
 }
@@ -154,6 +155,21 @@ __device__ __forceinline__ void fetch_interior(T* slot, const T* row, long long 
   for (int k = 0; k < NF; ++k) cp_async<V * (int)sizeof(T)>(slot + k * kIn, row + k * plane);
   cp_async_commit();
 }
+// The bounds-checked build checks each row against the grid (a separate function: handing
+// the grid to the unchecked one changes the register allocation of the lean loops).
+#ifdef LE2D_CHECK
+template <typename T, int V>
+__device__ __forceinline__ void fetch_interior_checked(T* slot, const T* row, const GridRef<T>& g) {
+  constexpr int kIn = 32 * V;
+#pragma unroll
+  for (int k = 0; k < NF; ++k)
+    if (in_src(g, row + k * g.plane, V)) cp_async<V * (int)sizeof(T)>(slot + k * kIn, row + k * g.plane);
+  cp_async_commit();
+}
+#define LE2D_FETCH_INTERIOR(T, V, slot, row, g) fetch_interior_checked<T, V>(slot, row, g)
+#else
+#define LE2D_FETCH_INTERIOR(T, V, slot, row, g) fetch_interior<T, V>(slot, row, (g).plane)
+#endif
 
 // `cy`: the y-sweep constants (Sweep, or YPairs for the FP32 pipeline).
 template <typename T, int V, int NPF, typename CY>
@@ -181,7 +197,7 @@ __device__ __forceinline__ bool pair_produce_interior(const GridRef<T>& g, const
   const T* next = g.src + (long long)(y0 - 4) * g.pitch + xs + lane * V;  // next row to fetch
 #pragma unroll
   for (int j = 0; j < NPF - 1; ++j) {
-    fetch_interior<T, V>(in_ring + j * kRow, next, g.plane);
+    LE2D_FETCH_INTERIOR(T, V, in_ring + j * kRow, next, g);
     next += g.pitch;
   }
   int aslot = 0;
@@ -189,7 +205,7 @@ __device__ __forceinline__ bool pair_produce_interior(const GridRef<T>& g, const
   bool ok = true;
   for (int m = y0 - 4; m < mend; ++m) {
     if (m + NPF - 1 < mend) {
-      fetch_interior<T, V>(in_ring + (islot == 0 ? NPF - 1 : islot - 1) * kRow, next, g.plane);
+      LE2D_FETCH_INTERIOR(T, V, in_ring + (islot == 0 ? NPF - 1 : islot - 1) * kRow, next, g);
       next += g.pitch;
     } else {
       cp_async_commit();  // keep one group per row
@@ -260,7 +276,7 @@ __device__ __forceinline__ bool pair_consume_interior(const GridRef<T>& g, const
       T gb[NF][V];
       ring_output(yb, gb, b_ring, bslot, cy);
 #pragma unroll
-      for (int k = 0; k < NF; ++k) store_if(writer, reinterpret_cast<VT*>(out + k * g.plane), pack(gb[k]));
+      for (int k = 0; k < NF; ++k) store_if(writer && in_dst(g, out + k * g.plane, V), reinterpret_cast<VT*>(out + k * g.plane), pack(gb[k]));
       out += g.pitch;
     }
     yb.right(cy);
@@ -299,14 +315,14 @@ __device__ __forceinline__ void march_tile_interior(const GridRef<T>& g, const S
   const T* next = g.src + (long long)(y0 - 2) * g.pitch + xs + lane * V;  // next row to fetch
 #pragma unroll
   for (int j = 0; j < NPF - 1; ++j) {
-    fetch_interior<T, V>(in_ring + j * kRow, next, g.plane);
+    LE2D_FETCH_INTERIOR(T, V, in_ring + j * kRow, next, g);
     next += g.pitch;
   }
   T* out = g.dst + (long long)y0 * g.pitch + xs + lane * V;  // next row written
   int islot = 0, xslot = 0;
   for (int m = y0 - 2; m < mend; ++m) {
     if (m + NPF - 1 < mend) {
-      fetch_interior<T, V>(in_ring + (islot == 0 ? NPF - 1 : islot - 1) * kRow, next, g.plane);
+      LE2D_FETCH_INTERIOR(T, V, in_ring + (islot == 0 ? NPF - 1 : islot - 1) * kRow, next, g);
       next += g.pitch;
     } else {
       cp_async_commit();  // keep one group per row
@@ -321,7 +337,7 @@ __device__ __forceinline__ void march_tile_interior(const GridRef<T>& g, const S
       T gf[NF][V];
       ring_output(yp, gf, xs_ring, xslot, c.y);
 #pragma unroll
-      for (int k = 0; k < NF; ++k) store_if(writer, reinterpret_cast<VT*>(out + k * g.plane), pack(gf[k]));
+      for (int k = 0; k < NF; ++k) store_if(writer && in_dst(g, out + k * g.plane, V), reinterpret_cast<VT*>(out + k * g.plane), pack(gf[k]));
       out += g.pitch;
     }
     yp.right(c.y);
@@ -460,7 +476,7 @@ __device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepCons
       mbar_arrive(empty + hs);
       T* out = g.dst + (long long)ka * g.pitch + col0;
 #pragma unroll
-      for (int k = 0; k < NF; ++k) store_if(writer, reinterpret_cast<VT*>(out + k * g.plane), pack(fa[k]));
+      for (int k = 0; k < NF; ++k) store_if(writer && in_dst(g, out + k * g.plane, V), reinterpret_cast<VT*>(out + k * g.plane), pack(fa[k]));
       ++u;
       continue;
     }
@@ -477,7 +493,7 @@ __device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepCons
         const int row = bin - 2;
         T* out = g.dst + (long long)row * g.pitch + col0;
 #pragma unroll
-        for (int k = 0; k < NF; ++k) store_if(writer, reinterpret_cast<VT*>(out + k * g.plane), pack(gb[k]));
+        for (int k = 0; k < NF; ++k) store_if(writer && in_dst(g, out + k * g.plane, V), reinterpret_cast<VT*>(out + k * g.plane), pack(gb[k]));
         if (TAP && row == tap_b.row && writer) tap_row<T, V>(tap_b, g.pitch, col0, gb);
       }
       yb.right(c.y);

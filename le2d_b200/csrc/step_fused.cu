@@ -413,6 +413,18 @@ cudaError_t launch_fused_step(const T* src, T* dst, int nx, int ny, long long pi
                               &lo, &hi, s);
 }
 
+#ifdef LE2D_CHECK
+unsigned long long check_violations_fused() {
+  unsigned long long v = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&v, march::g_check_violations, sizeof(v)) != cudaSuccess ||
+      cudaMemcpyToSymbol(march::g_check_violations, &zero, sizeof(zero)) != cudaSuccess) {
+    cudaGetLastError();
+    return ~0ULL;  // unreadable: reported as violations
+  }
+  return v;
+}
+#endif
+
 #define LE2D_INST(T)                                                                            \
   template int fused_variant_count<T>();                                                        \
   template int fused_variant_lanes<T>(int);                                                     \
