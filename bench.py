@@ -24,7 +24,9 @@ Our arm (default) prints one JSON line with
             same GPU: solves/s of both, the speed-up, and the FP32 fields of every instance
             against the FP64 library's (which equals the reference double build),
   serving   Poisson request streams (10 and 200 requests/s) through the serving loop:
-            solves/s and p50/p99 latency beside a one-at-a-time plain le_step server.
+            solves/s and p50/p99 latency beside a one-at-a-time plain le_step server,
+  precision 4096x4096 with disks and noise, 4000 steps: FP32 against FP64 (= the reference
+            double build) per field every 500 steps, and the FP64 energy drift.
 Under torchrun each rank solves its own instance (independent solves, weak scaling);
 value is the total node-updates of all ranks over the slowest rank's time; the batched
 and serving measurements run only in the one-process case.
@@ -764,9 +766,11 @@ def run_dist(args):
     return 0
 
 
-def run_precision(args):
-    """4096x4096 precision study: FP32 vs FP64 library every 500 steps up to 4000 steps,
-    FP64 energy drift, and both builds against the reference's own CPU builds after 500 steps."""
+def precision_measure(args, with_reference=True):
+    """4096x4096 precision study: FP32 vs FP64 library every 500 steps up to 4000 steps (the
+    FP64 library equals the reference double build value for value, so this is also FP32 vs
+    the reference double build), FP64 energy drift; with_reference: both builds against the
+    reference's own CPU builds after 500 steps (~2 min of host time)."""
     from oracle.oracle import Reference, aos_to_soa, fields, max_abs, rel_l2
 
     p = workloads.precision_4096()
@@ -796,7 +800,7 @@ def run_precision(args):
             g = np.zeros(5 * n * n, lib.dtype)
             assert lib.download(tasks[prec], g) == 0
             out[prec] = fields(g, n, n, 1)
-            if k == 1:
+            if k == 1 and with_reference:
                 snap[prec] = g
         ed = libs["d"].diagnostics(tasks["d"])[1]["energy"]
         ef = libs["f"].diagnostics(tasks["f"])[1]["energy"]
@@ -812,7 +816,7 @@ def run_precision(args):
             "every": 500, "rows": rows}
     # the reference's own CPU builds (simple/, OpenMP on all host cores) from the same initial
     # states for the first 500 steps, against the library's FP64 / FP32 results at step 500
-    if Reference.available("d") and not args.no_cpu:
+    if Reference.available("d") and with_reference:
         threads = os.cpu_count() or 1
         for prec in ("d", "f"):
             ref = Reference(prec)
@@ -827,7 +831,11 @@ def run_precision(args):
                 ref_d = fr
         line["step500_reference_f_vs_reference_d_rel_l2"] = rel_l2(fr, ref_d).tolist()
         line["reference_threads"] = threads
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_precision(args):
+    print(json.dumps(precision_measure(args, with_reference=not args.no_cpu)), flush=True)
     return 0
 
 
@@ -969,6 +977,7 @@ def main():
         # the batched and serving targets on the same GPU (one process; skipped under torchrun)
         line["batched"] = batched_measure(args)
         line["serving"] = serving_measure(args, [float(r) for r in args.extra_rates.split(",")])
+        line["precision"] = precision_measure(args, with_reference=False)
     if rank == 0 and not args.no_cpu:
         cb = cpu_reference_sample(p)
         line["cpu_baseline"] = cb["simple"]
