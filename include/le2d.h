@@ -166,8 +166,9 @@ int le2d_batch_set_wait_limit(le2d_batch *b, unsigned long long ns);
  * nx x ny nodes (enough copies for ~24 M nodes) for every tile height (16 ... 256 rows) and
  * steps per work item (1, and 2 -- a producer / consumer warp pair per tile -- in the FP32
  * library), and keeps the fastest for the size class (nx, ny rounded up to powers of two).
- * Instances of a tuned class that are added to a batch or a server afterwards use it; with
- * LE2D_AUTOTUNE=1 le2d_batch_add tunes a class on its first instance.  out (may be NULL):
+ * Instances of a tuned class that are added to a batch afterwards use it (a server keeps the
+ * default tiles, which give small solves shorter latency); with LE2D_AUTOTUNE=1
+ * le2d_batch_add tunes a class on its first instance.  out (may be NULL):
  * {tile rows, steps per item}; *nu_per_s (may be NULL): the measured node-updates/s. */
 int le2d_batch_autotune(int nx, int ny, int *out, double *nu_per_s);
 /* Forgets every tuned size class of the batched path. */

@@ -266,7 +266,7 @@ int Engine<T>::alloc_instance(const le2d_problem& p, Inst& in) {
   // Tile height and steps per work item: explicit (autotuner trials), else the autotuner's
   // table for the size class (LE2D_AUTOTUNE=1 tunes a class on first use), else defaults.
   int seg = seg_len_, depth = batch_depth<T>();
-  if (!seg_set_ && !depth_set_) {
+  if (!seg_set_ && !depth_set_ && use_tuned_) {
     BatchTuned bt;
     bool have = batch_tuned(p.nx, p.ny, &bt);
     const char* a = getenv("LE2D_AUTOTUNE");

@@ -208,6 +208,7 @@ le2d_server* le2d_server_create(size_t device_budget_bytes, int window_steps, in
     delete s;
     return nullptr;
   }
+  s->eng->set_use_tuned(false);  // default tiles: shorter chains per small solve (engine.h)
   s->window = window_steps;
   s->max_active = max_active;
   int dev = 0;
