@@ -32,6 +32,9 @@
 // rows as they are.
 // A producer may claim its next item while its consumer still finishes the last one: all
 // rows of that item are already in the queue, so the consumer finishes without it.
+// The x-sweep runs one invariant at a time (sweep_x_lane_diff), which at this kernel's
+// occupancy is faster than the packed form the single-solve kernels use; both give the
+// same bits.
 #include <type_traits>
 
 #include "march_pair.cuh"
@@ -144,7 +147,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
     const long long step_after = I.abs_step0 + r + 1;  // absolute step count after this step
     if (I.trace != nullptr && step_after % I.trace_every == 0)
       tap = march::RowTap<T>{I.trace + (step_after / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
-    march::march_tile<T, V, kNpf, true, true>(g, I.c, bt.strip, y0, y1, ring, tap);
+    march::march_tile<T, V, kNpf, true, true, false>(g, I.c, bt.strip, y0, y1, ring, tap);
     __syncwarp();
     const int tile_id = I.tile_base + bt.seg * I.nstrips + bt.strip;
     if (lane == 0 && !(r == 0 && tile_id == stall_plus1 - 1)) {
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
       const march::GridRef<T> g{I.buf[par], I.buf[par ^ 1], I.nx, I.ny, I.pitch, I.plane, I.far_rot};
       const int y0 = bt.seg * I.seg_len;
       const int y1 = min(y0 + I.seg_len, I.ny);
-      if (!march::pair_produce<T, V, kNpf, true>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
+      if (!march::pair_produce<T, V, kNpf, true, false>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
                                                  u, nadv == 1))
         break;
     }
@@ -237,7 +240,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
       if (I.trace != nullptr && nadv == 2 && (before + 2) % I.trace_every == 0)
         tap_b = march::RowTap<T>{I.trace + ((before + 2) / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
       const int tile_id = I.tile_base + bt.seg * I.nstrips + bt.strip;
-      if (!march::pair_consume<T, V, kNpf, true>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
+      if (!march::pair_consume<T, V, kNpf, true, false>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
                                                  u, nadv == 1, tap_a, tap_b))
         break;
       __syncwarp();  // the consumer wrote the tile's new state and publishes it
@@ -251,8 +254,8 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
 
 template <typename T>
 struct BatchKernelOf;
-// FP32: two-step items on warp pairs (4 columns per lane, 16 warps per SM); FP64: one-step
-// items on single warps (2 columns per lane).
+// FP32: two-step items on warp pairs (4 columns per lane, 168 registers: 12 warps per SM);
+// FP64: one-step items on single warps (2 columns per lane, 8 warps per SM).
 template <>
 struct BatchKernelOf<float> {
   static constexpr int V = 4, MINB = 3, DEPTH = 2;

@@ -28,6 +28,14 @@ inline Sweep<real> make_sweep(real dt, const le_material& m, real h) {
   s.rhoc1 = m.rhoc1;
   s.rhoc2 = m.rhoc2;
   s.rhoc3 = m.rhoc3;
+  s.irp.x = s.irhoc1;
+  s.irp.y = s.irhoc2;
+  s.nirp.x = -s.irhoc1;
+  s.nirp.y = -s.irhoc2;
+  s.kcp.x = s.kc1;
+  s.kcp.y = s.kc2;
+  s.nkcp.x = -s.kc1;
+  s.nkcp.y = -s.kc2;
   return s;
 }
 

@@ -38,6 +38,11 @@ namespace le2d {
 
 enum Field { VX = 0, VY = 1, SXX = 2, SXY = 3, SYY = 4, NF = 5 };
 
+template <typename T>
+struct Pair;
+template <> struct Pair<float> { using type = float2; };
+template <> struct Pair<double> { using type = double2; };
+
 // Constants of one directional sweep (built on the host by make_sweep()).
 template <typename T>
 struct Sweep {
@@ -47,6 +52,10 @@ struct Sweep {
   T hk1rc1, hk1rc3, hk2rc2;  // k1/2 * rhoc1, k1/2 * rhoc3, k2/2 * rhoc2
   T k1, k2;                  // Courant numbers dt*c/h (plain per-node scheme)
   T rhoc1, rhoc2, rhoc3;     // the material's products (plain per-node scheme)
+  // (irhoc1, irhoc2), (-irhoc1, -irhoc2), (kc1, kc2), (-kc1, -kc2): the operands of the
+  // packed FP32 x-sweep, which works on the invariant pairs (w1, w3) and (w2, w4); as
+  // aligned pairs in the kernel parameters a packed instruction takes each as one operand.
+  typename Pair<T>::type irp, nirp, kcp, nkcp;
 };
 
 template <typename T>

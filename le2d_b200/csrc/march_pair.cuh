@@ -350,7 +350,7 @@ __device__ __forceinline__ void march_tile_interior(const GridRef<T>& g, const S
 // the consumer; `u` counts the queue's handoffs (it continues across tiles).  A one_step
 // tile (an odd last step, or le_step_soa's far end, which g.far_rot selects) hands over
 // step A's rows [y0, y1) only, which the consumer writes.  Returns false if a wait gave up.
-template <typename T, int V, int NPF, bool COHERENT>
+template <typename T, int V, int NPF, bool COHERENT, bool XPACK = true>
 __device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepConsts<T>& c, int strip,
                                              int y0, int y1, T* smem_pair,
                                              unsigned long long* bars,
@@ -399,7 +399,7 @@ __device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepCons
 #pragma unroll
     for (int k = 0; k < NF; ++k)
       unpack(*reinterpret_cast<const VT*>(in_ring + islot * kRow + k * kIn), f[k]);
-    sweep_x_lane<T, V>(f, c.x);
+    sweep_x_lane<T, V, XPACK>(f, c.x);
     ring_left(ya, f, a_ring, aslot, c.y);
     const int ka = m - 2;  // step-A row completed now
     if (m >= y0 && row_uses(ka, y0, y1, g.ny, one_step) > 0) {
@@ -430,7 +430,7 @@ __device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepCons
 // producer.  A one_step tile's handed rows are step A's rows [y0, y1), written as they
 // are.  TAP: receiver rows -- tap_a of the rows after step A (taken from the handed rows),
 // tap_b of the rows after step B.  Returns false if a wait gave up.
-template <typename T, int V, int NPF, bool TAP>
+template <typename T, int V, int NPF, bool TAP, bool XPACK = true>
 __device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepConsts<T>& c, int strip,
                                              int y0, int y1, T* smem_pair,
                                              unsigned long long* bars,
@@ -485,7 +485,7 @@ __device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepCons
 #pragma unroll
       for (int k = 0; k < NF; ++k) unpack(*reinterpret_cast<const VT*>(slot + k * kIn), fb[k]);
       if (r == reps - 1) mbar_arrive(empty + hs);
-      sweep_x_lane<T, V>(fb, c.x);
+      sweep_x_lane<T, V, XPACK>(fb, c.x);
       ring_left(yb, fb, b_ring, bslot, c.y);
       if (bin >= y0 + 2) {  // step-B row bin-2 is complete
         T gb[NF][V];
