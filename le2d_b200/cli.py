@@ -11,6 +11,14 @@ optionally save the VTK.  The default initial condition is the reference driver'
 uses the seeded 8-disk material of the 8192x8192 workload scaled to the grid.
 --variant / --seg pick a compiled fused-kernel variant and row-segment length
 (le2d_set_variant) and print the plan, e.g. to profile one kernel variant.
+
+    python -m le2d_b200.cli batch n steps [--window W] [--tune]
+
+runs the first n instances of the seeded 256-instance mix (bench.py's batched workload:
+sides 128-2048, their own materials and disks), `steps` steps each, through the batched
+path (le2d_batch_*, windows of W steps; --tune: the batched autotuner's tiles per size
+class, else the default tiles) and prints the launch rate, e.g. to profile the batched
+kernel on a small case.
 """
 from __future__ import annotations
 
@@ -21,7 +29,38 @@ import time
 from le2d_b200 import capi, workloads
 
 
+def main_batch(argv) -> int:
+    ap = argparse.ArgumentParser(prog="cli batch")
+    ap.add_argument("n", type=int, help="instances: the first n of the 256-instance mix")
+    ap.add_argument("steps", type=int, help="steps of every instance")
+    ap.add_argument("--window", type=int, default=256, help="steps per persistent launch")
+    ap.add_argument("--tune", action="store_true", help="batched autotuner's tiles per size class")
+    a = ap.parse_args(argv)
+    lib = capi.Lib("f")
+    probs = [workloads.Problem(**{**p.__dict__, "steps": a.steps}) for p in workloads.batched_256()[:a.n]]
+    budget = int(1.1 * sum(2 * 5 * 4 * (((p.nx + 31) // 32) * 32) * p.ny + 512 for p in probs)) + (64 << 20)
+    if a.tune:
+        lib.batch_autotune_reset()
+        for p in probs:
+            lib.batch_autotune(p.nx, p.ny)
+    with capi.Batch(lib, budget) as b:
+        for p in probs:
+            if b.add(b.problem(p), disks=p.disks) < 0:
+                print("le2d_batch_add failed", file=sys.stderr)
+                return 1
+        rc, ms = b.run(window_steps=a.window)
+    if rc != 0:
+        print(f"le2d error: {lib.strerror(rc)}", file=sys.stderr)
+        return 1
+    nu = sum(p.nx * p.ny for p in probs) * a.steps
+    print(f"{len(probs)} instances {a.steps} steps {ms:.2f} ms {nu / (ms * 1e-3):.4g} nu/s")
+    return 0
+
+
 def main(argv=None) -> int:
+    argv = sys.argv[1:] if argv is None else argv
+    if argv and argv[0] == "batch":
+        return main_batch(argv[1:])
     ap = argparse.ArgumentParser()
     ap.add_argument("nx", type=int)
     ap.add_argument("ny", type=int)

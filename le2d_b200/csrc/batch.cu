@@ -157,6 +157,38 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
   }
 }
 
+// The sweep constants of the item a warp of a pair works on, copied from the instance record
+// into the warp's own slot of shared memory when it starts the item: the march reads them
+// every row, and the record lives in global memory (the single-solve kernels take them from
+// the kernel parameters instead).  The y-sweep's come as the pairs the packed y-pipeline
+// multiplies by.
+template <typename T>
+struct ItemConsts {
+  Sweep<T> x;
+  YPairs y;
+};
+template <typename T>
+__host__ __device__ constexpr int item_consts_bytes() { return ((int)sizeof(ItemConsts<T>) + 15) / 16 * 16; }
+
+// Shared memory of one pair of the batched kernel: the march's, then one ItemConsts slot
+// per warp.
+template <typename T, int V>
+__host__ __device__ constexpr int batch_pair_bytes() { return march::pair_smem_bytes<T, V, kNpf>() + 2 * item_consts_bytes<T>(); }
+
+template <typename T>
+__device__ __forceinline__ const ItemConsts<T>& load_item_consts(ItemConsts<T>* slot, const BatchInst<T>& I) {
+  constexpr int kx = (int)(sizeof(Sweep<T>) / 4), ky = (int)(sizeof(YPairs) / 4);
+  const int lane = threadIdx.x & 31;
+  const unsigned* sx = reinterpret_cast<const unsigned*>(&I.c.x);
+  const unsigned* sy = reinterpret_cast<const unsigned*>(&I.yq);
+  unsigned* dx = reinterpret_cast<unsigned*>(&slot->x);
+  unsigned* dy = reinterpret_cast<unsigned*>(&slot->y);
+  for (int i = lane; i < kx; i += 32) dx[i] = sx[i];
+  for (int i = lane; i < ky; i += 32) dy[i] = sy[i];
+  __syncwarp();
+  return *slot;
+}
+
 template <typename T, int V, int MINB>
 __global__ void __launch_bounds__(kWarps * 32, MINB)
     batch_pair_kernel(const BatchInst<T>* __restrict__ insts, const BatchTile* __restrict__ tiles,
@@ -167,8 +199,10 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const bool producer = (wib & 1) == 0;
-  unsigned char* base = smem_raw + (wib >> 1) * march::pair_smem_bytes<T, V, kNpf>();
+  unsigned char* base = smem_raw + (wib >> 1) * batch_pair_bytes<T, V>();
   T* smem = reinterpret_cast<T*>(base);
+  ItemConsts<T>* kslot = reinterpret_cast<ItemConsts<T>*>(base + march::pair_smem_bytes<T, V, kNpf>() +
+                                                          (wib & 1) * item_consts_bytes<T>());
   unsigned long long* bars =
       reinterpret_cast<unsigned long long*>(base + march::pair_smem_elems<T, V, kNpf>() * sizeof(T));
   volatile long long* item_q = reinterpret_cast<volatile long long*>(bars + 2 * kHand);
@@ -208,8 +242,9 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
       const march::GridRef<T> g{I.buf[par], I.buf[par ^ 1], I.nx, I.ny, I.pitch, I.plane, I.far_rot};
       const int y0 = bt.seg * I.seg_len;
       const int y1 = min(y0 + I.seg_len, I.ny);
-      if (!march::pair_produce<T, V, kNpf, true, false>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
-                                                 u, nadv == 1))
+      const ItemConsts<T>& k = load_item_consts(kslot, I);
+      if (!march::pair_produce<T, V, kNpf, true, false>(g, k.x, k.y, bt.strip, y0, y1, smem, bars, wait_ns,
+                                                        status, u, nadv == 1))
         break;
     }
   } else {
@@ -240,8 +275,9 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
       if (I.trace != nullptr && nadv == 2 && (before + 2) % I.trace_every == 0)
         tap_b = march::RowTap<T>{I.trace + ((before + 2) / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
       const int tile_id = I.tile_base + bt.seg * I.nstrips + bt.strip;
-      if (!march::pair_consume<T, V, kNpf, true, false>(g, I.c, bt.strip, y0, y1, smem, bars, wait_ns, status,
-                                                 u, nadv == 1, tap_a, tap_b))
+      const ItemConsts<T>& k = load_item_consts(kslot, I);
+      if (!march::pair_consume<T, V, kNpf, true, false>(g, k.x, k.y, bt.strip, y0, y1, smem, bars, wait_ns,
+                                                        status, u, nadv == 1, tap_a, tap_b))
         break;
       __syncwarp();  // the consumer wrote the tile's new state and publishes it
       if (lane == 0 && !(r == 0 && tile_id == stall_plus1 - 1)) {
@@ -260,7 +296,7 @@ template <>
 struct BatchKernelOf<float> {
   static constexpr int V = 4, MINB = 3, DEPTH = 2;
   static void* fn() { return (void*)batch_pair_kernel<float, V, MINB>; }
-  static size_t smem() { return (size_t)(kWarps / 2) * march::pair_smem_bytes<float, V, kNpf>(); }
+  static size_t smem() { return (size_t)(kWarps / 2) * batch_pair_bytes<float, V>(); }
 };
 template <>
 struct BatchKernelOf<double> {

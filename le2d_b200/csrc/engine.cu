@@ -1,6 +1,7 @@
 // Batched solves: instance states in a device arena, per-window work lists for the
 // persistent kernel (batch.cu), CUDA-graph capture of the window loop, read-back.
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -416,6 +417,8 @@ typename Engine<T>::Window Engine<T>::plan_window(int window, const std::vector<
     b.pitch = in.pitch;
     b.plane = in.plane;
     b.c = in.c;
+    b.yq = YPairs{};
+    if constexpr (std::is_same<T, float>::value) b.yq = make_ypairs(in.c.y);
     b.far_rot = in.p.stype == ST_SOA;
     b.nstrips = in.nstrips;
     b.nsegs = in.nsegs;

@@ -111,6 +111,7 @@ struct BatchInst {
   int nx, ny;
   long long pitch, plane;
   StepConsts<T> c;
+  YPairs yq;             // FP32: c.y as pairs for the packed y-pipeline
   int far_rot;           // le_step_soa far-end rows
   int nstrips, nsegs, seg_len;
   int tile_base;         // index of the instance's first tile in the tile list and done[]

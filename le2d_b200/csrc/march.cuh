@@ -133,30 +133,6 @@ __device__ __forceinline__ int source_row(int m, int ny, int far_rot) {
   return far_rot ? max(m - 5, 0) : ny - 1;
 }
 
-template <typename T, int V, bool COHERENT>
-__device__ __forceinline__ void load_row(T (&f)[NF][V], const GridRef<T>& g, int row, int col0,
-                                         bool interior) {
-  using VT = typename Vec<T, V>::type;
-  const T* base = g.src + (long long)row * g.pitch;
-  if (interior) {
-#pragma unroll
-    for (int k = 0; k < NF; ++k) {
-      const T* p = base + k * g.plane + col0;
-      unpack(in_src(g, p, V) ? load_state<COHERENT>(reinterpret_cast<const VT*>(p)) : VT{}, f[k]);
-    }
-  } else {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const int cc = min(max(col0 + v, 0), g.nx - 1);
-#pragma unroll
-      for (int k = 0; k < NF; ++k) {
-        const T* p = base + k * g.plane + cc;
-        f[k][v] = in_src(g, p, 1) ? load_state<COHERENT>(p) : T(0);
-      }
-    }
-  }
-}
-
 // FP64 x-sweep in the reference's flux form (tvd2, simple/le_core.c:48-69): invariants
 // w of each node, face differences D = w_{i+1} - w_i, slope ratios, limited fluxes
 // F_i = w_i + psi_i D_i (right-moving w1, w3) and G_i = w_i - psi'_i D_{i-1} (left-moving
@@ -449,31 +425,53 @@ __device__ __forceinline__ void store_if(bool p, double* a, const double& v) {
                : "memory");
 }
 
-// Starts copying source row `row` into this lane's slot of the input ring.  Strips that
-// reach past the grid edge load their clamped columns synchronously instead.
+// Element i of a lane's V values (a select chain: i is not a compile-time index).
+template <typename T, int V>
+__device__ __forceinline__ T pick(const T (&a)[V], int i) {
+  T s = a[0];
+#pragma unroll
+  for (int j = 1; j < V; ++j) s = i == j ? a[j] : s;
+  return s;
+}
+
+// The first column of the aligned V-column chunk a lane of a strip that reaches past the
+// grid edge copies: its own columns clamped into [0, nx) all lie in it, and it lies inside
+// the row's pitch (rows are padded to whole chunks).
+template <int V>
+__device__ __forceinline__ int chunk_col(int col0, int nx) {
+  return min(max(col0, 0), (nx - 1) / V * V);
+}
+
+// Starts copying source row `row` into this lane's slot of the input ring.  A strip that
+// reaches past the grid edge copies each lane's chunk_col() chunk instead; clamp_lane()
+// then gives the lane's columns outside [0, nx) the values of column 0 / nx-1.
 template <typename T, int V, bool COHERENT>
 __device__ __forceinline__ void fetch_row(T* slot, const GridRef<T>& g, int row, int col0,
                                           bool interior) {
   constexpr int kIn = 32 * V;
-  const T* base = g.src + (long long)row * g.pitch;
-  if (interior) {
+  const T* base = g.src + (long long)row * g.pitch + (interior ? col0 : chunk_col<V>(col0, g.nx));
 #pragma unroll
-    for (int k = 0; k < NF; ++k) {
-      const T* p = base + k * g.plane + col0;
-      if (in_src(g, p, V)) cp_async<V * (int)sizeof(T)>(slot + k * kIn, p);
-    }
-  } else {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const int cc = min(max(col0 + v, 0), g.nx - 1);
-#pragma unroll
-      for (int k = 0; k < NF; ++k) {
-        const T* p = base + k * g.plane + cc;
-        slot[k * kIn + v] = in_src(g, p, 1) ? load_state<COHERENT>(p) : T(0);
-      }
-    }
+  for (int k = 0; k < NF; ++k) {
+    const T* p = base + k * g.plane;
+    if (in_src(g, p, V)) cp_async<V * (int)sizeof(T)>(slot + k * kIn, p);
   }
   cp_async_commit();
+}
+
+// The lane's values of a row fetched from its chunk_col() chunk, as the clamped columns
+// col0 .. col0+V-1: its own columns where the chunk starts at col0 (positions up to nx-1),
+// the chunk's column 0 (left of the grid) or nx-1 (right of it) for the others.
+template <typename T, int V>
+__device__ __forceinline__ void clamp_lane(T (&f)[NF][V], int col0, int nx) {
+  const int c0 = chunk_col<V>(col0, nx);
+  const int last = col0 < 0 ? 0 : min(nx - 1 - c0, V - 1);  // position of the edge column
+  const int keep = c0 == col0 ? last : -1;                   // own columns: positions [0, keep]
+#pragma unroll
+  for (int k = 0; k < NF; ++k) {
+    const T e = pick<T, V>(f[k], last);
+#pragma unroll
+    for (int v = 0; v < V; ++v) f[k][v] = v <= keep ? f[k][v] : e;
+  }
 }
 
 // The per-column y-pipeline.  Row m arrives x-swept; with row m-1 it gives the face
@@ -707,6 +705,7 @@ __device__ __forceinline__ void march_tile(const GridRef<T>& g, const StepConsts
 #pragma unroll
     for (int k = 0; k < NF; ++k)
       unpack(*reinterpret_cast<const VT*>(in_ring + islot * kRow + k * kIn), f[k]);
+    if (!interior) clamp_lane<T, V>(f, col0, g.nx);
 
     sweep_x_lane<T, V, XPACK>(f, c.x);
 

@@ -29,14 +29,6 @@ __host__ __device__ constexpr int warp_smem_elems2() {
   return (6 + NPF) * NF * 32 * V;  // input ring + step A ring + step B ring
 }
 
-template <typename T, int V>
-__device__ __forceinline__ T pick(const T (&a)[V], int i) {
-  T s = a[0];
-#pragma unroll
-  for (int j = 1; j < V; ++j) s = i == j ? a[j] : s;
-  return s;
-}
-
 // Columns of this lane outside [0, nx) take the values of column 0 / column nx-1, which
 // the strip holds (lane (c - xs) / V, position (c - xs) % V).
 template <typename T, int V>
@@ -141,6 +133,7 @@ __device__ __forceinline__ void march_tile2(const GridRef<T>& g, const StepConst
 #pragma unroll
     for (int k = 0; k < NF; ++k)
       unpack(*reinterpret_cast<const VT*>(in_ring + islot * kRow + k * kIn), f[k]);
+    if (!interior) clamp_lane<T, V>(f, col0, g.nx);
     sweep_x_lane<T, V>(f, c.x);
     ring_left(ya, f, a_ring, aslot, c.y);
 

@@ -350,8 +350,8 @@ __device__ __forceinline__ void march_tile_interior(const GridRef<T>& g, const S
 // the consumer; `u` counts the queue's handoffs (it continues across tiles).  A one_step
 // tile (an odd last step, or le_step_soa's far end, which g.far_rot selects) hands over
 // step A's rows [y0, y1) only, which the consumer writes.  Returns false if a wait gave up.
-template <typename T, int V, int NPF, bool COHERENT, bool XPACK = true>
-__device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepConsts<T>& c, int strip,
+template <typename T, int V, int NPF, bool COHERENT, bool XPACK = true, typename CY = Sweep<T>>
+__device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const Sweep<T>& cx, const CY& cy, int strip,
                                              int y0, int y1, T* smem_pair,
                                              unsigned long long* bars,
                                              unsigned long long wait_ns, int* status, unsigned& u,
@@ -399,12 +399,13 @@ __device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepCons
 #pragma unroll
     for (int k = 0; k < NF; ++k)
       unpack(*reinterpret_cast<const VT*>(in_ring + islot * kRow + k * kIn), f[k]);
-    sweep_x_lane<T, V, XPACK>(f, c.x);
-    ring_left(ya, f, a_ring, aslot, c.y);
+    if (!interior) clamp_lane<T, V>(f, col0, g.nx);
+    sweep_x_lane<T, V, XPACK>(f, cx);
+    ring_left(ya, f, a_ring, aslot, cy);
     const int ka = m - 2;  // step-A row completed now
     if (m >= y0 && row_uses(ka, y0, y1, g.ny, one_step) > 0) {
       T ga[NF][V];
-      ring_output(ya, ga, a_ring, aslot, c.y);
+      ring_output(ya, ga, a_ring, aslot, cy);
       if (!interior) clamp_columns<T, V>(ga, xs, col0, g.nx);
       const int hs = (int)(u % kHand);
       const unsigned use = u / kHand;
@@ -418,7 +419,7 @@ __device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepCons
       mbar_arrive(full + hs);
       ++u;
     }
-    ya.right(c.y);
+    ya.right(cy);
     islot = islot + 1 == NPF ? 0 : islot + 1;
     aslot = aslot == 2 ? 0 : aslot + 1;
   }
@@ -430,8 +431,8 @@ __device__ __forceinline__ bool pair_produce(const GridRef<T>& g, const StepCons
 // producer.  A one_step tile's handed rows are step A's rows [y0, y1), written as they
 // are.  TAP: receiver rows -- tap_a of the rows after step A (taken from the handed rows),
 // tap_b of the rows after step B.  Returns false if a wait gave up.
-template <typename T, int V, int NPF, bool TAP, bool XPACK = true>
-__device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepConsts<T>& c, int strip,
+template <typename T, int V, int NPF, bool TAP, bool XPACK = true, typename CY = Sweep<T>>
+__device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const Sweep<T>& cx, const CY& cy, int strip,
                                              int y0, int y1, T* smem_pair,
                                              unsigned long long* bars,
                                              unsigned long long wait_ns, int* status, unsigned& u,
@@ -485,18 +486,18 @@ __device__ __forceinline__ bool pair_consume(const GridRef<T>& g, const StepCons
 #pragma unroll
       for (int k = 0; k < NF; ++k) unpack(*reinterpret_cast<const VT*>(slot + k * kIn), fb[k]);
       if (r == reps - 1) mbar_arrive(empty + hs);
-      sweep_x_lane<T, V, XPACK>(fb, c.x);
-      ring_left(yb, fb, b_ring, bslot, c.y);
+      sweep_x_lane<T, V, XPACK>(fb, cx);
+      ring_left(yb, fb, b_ring, bslot, cy);
       if (bin >= y0 + 2) {  // step-B row bin-2 is complete
         T gb[NF][V];
-        ring_output(yb, gb, b_ring, bslot, c.y);
+        ring_output(yb, gb, b_ring, bslot, cy);
         const int row = bin - 2;
         T* out = g.dst + (long long)row * g.pitch + col0;
 #pragma unroll
         for (int k = 0; k < NF; ++k) store_if(writer && in_dst(g, out + k * g.plane, V), reinterpret_cast<VT*>(out + k * g.plane), pack(gb[k]));
         if (TAP && row == tap_b.row && writer) tap_row<T, V>(tap_b, g.pitch, col0, gb);
       }
-      yb.right(c.y);
+      yb.right(cy);
       bslot = bslot == 2 ? 0 : bslot + 1;
       ++bin;
     }

@@ -148,10 +148,10 @@ __global__ void __launch_bounds__(W * 32, MINB) fused_pair_kernel(const FusedPar
     }
   }
   if (producer)
-    march::pair_produce<T, V, NPF, false>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns,
+    march::pair_produce<T, V, NPF, false>(p.g, p.c.x, ycons(p), strip, y0, y1, smem, bars, p.pair.wait_ns,
                                           p.pair.status, u, false);
   else
-    march::pair_consume<T, V, NPF, false>(p.g, p.c, strip, y0, y1, smem, bars, p.pair.wait_ns,
+    march::pair_consume<T, V, NPF, false>(p.g, p.c.x, ycons(p), strip, y0, y1, smem, bars, p.pair.wait_ns,
                                           p.pair.status, u, false, no_tap, no_tap);
 }
 

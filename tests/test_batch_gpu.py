@@ -231,3 +231,13 @@ def test_batch_odd_windows_and_receivers(libs, prec):
             rec = b.receivers(i)
             assert rec.shape == (p.steps // 3, 2, p.nx)
             assert rec.tobytes() == samples.astype(lib.dtype).tobytes(), (i, st)
+
+
+def test_cli_batch_subcommand(capsys):
+    """`python -m le2d_b200.cli batch n steps` (the driver the batched kernel's profile is
+    taken with) runs the first n instances of the mix through the batched path."""
+    from le2d_b200 import cli
+
+    assert cli.main(["batch", "3", "6", "--window", "4"]) == 0
+    out = capsys.readouterr().out.split()
+    assert out[:4] == ["3", "instances", "6", "steps"] and float(out[-2]) > 0
