@@ -8,6 +8,7 @@
 // block is just kWarps of them sharing the launch.  Variants of temporal-block depth 2
 // advance each tile by two steps per launch, on one warp (march2.cuh) or on a producer /
 // consumer warp pair (march_pair.cuh).
+#include <cmath>
 #include <type_traits>
 
 #include "march_pair.cuh"
@@ -328,6 +329,42 @@ int fused_resident_warps(int device, int variant) {
 // at least twice min_seg (at 4096^2: 32-row segments 1.17e11, 16-row 1.09e11).
 constexpr int kWaves = 8;
 
+// The segment length L that minimises a model of the launch time fitted to measured
+// launches,
+//   time ~ (w + beta + alpha (ceil(w) - w)) (L + h),   w = tiles / resident tiles,
+// w being the launch's waves of tiles, L + h the rows of a tile's march (h for its halo rows
+// and the fill of its pipeline) and the idle part of the last wave charged at alpha.  Fits:
+//   warp-pair (two-step) variants, the FP32 default measured on grids 1024^2 to 16384^2,
+//   8192 x 2048 and 2048 x 8192 with segments of 32 to 256 rows: h = 6, beta = 0.2,
+//   alpha = 0.3 -- within 2 % of the fastest measured length on each of those grids but
+//   8192 x 2048 (3 %), where the 8-wave rule lost up to 6 % (158 against 168 Gnu/s on
+//   6000^2, 173 against 177 on 8192^2);
+//   FP64 one-step variants, the FP64 default measured on 2048^2 to 12000^2 with segments of
+//   16 to 128 rows: h = 2, beta = 0.1, alpha = 0.3 -- 42.5 against 40.3 Gnu/s on 2048^2,
+//   49.3 against 46.6 on 4096^2 under the 8-wave rule.
+// Lengths above 256 rows were not measured and are not considered.
+struct SegModel {
+  double h, beta, alpha;
+  int step;
+};
+constexpr SegModel kPairModel{6.0, 0.2, 0.3, 16};
+constexpr SegModel kStepModelF64{2.0, 0.1, 0.3, 8};
+
+inline int model_segment(const SegModel& m, int ny, int nstrips, int resident_tiles, int min_len) {
+  int best_len = min_len;
+  double best = 1e300;
+  for (int len = min_len; len <= 256 && len < ny + m.step; len += m.step) {
+    const int l = len < ny ? len : ny;
+    const double w = (double)nstrips * ((ny + l - 1) / l) / resident_tiles;
+    const double t = (w + m.beta + m.alpha * (std::ceil(w) - w)) * (l + m.h);
+    if (t < best) {
+      best = t;
+      best_len = l;
+    }
+  }
+  return best_len;
+}
+
 template <typename T>
 FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_seg) {
   FusedPlan pl;
@@ -342,6 +379,10 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
   if (target < 1) target = 1;
   int seg = (ny + target - 1) / target;
   if (seg < min_seg * pl.depth) seg = min_seg * pl.depth;
+  if (resident_tasks > 0 && pl.warps_per_task == 2)
+    seg = model_segment(kPairModel, ny, pl.nstrips, resident_tasks, min_seg * pl.depth);
+  else if (resident_tasks > 0 && sizeof(T) == 8 && pl.depth == 1)
+    seg = model_segment(kStepModelF64, ny, pl.nstrips, resident_tasks, min_seg);
   if (seg > ny) seg = ny;
   pl.seg_len = seg;
   pl.nsegs = (ny + seg - 1) / seg;
