@@ -252,6 +252,12 @@ size_t le2d_task_device_bytes(int nx, int ny);
  * division is the compiler's). */
 int le2d_selftest_ratio(const double *a, const double *b, long long n, double *fast, double *ieee);
 
+/* Self-test of the FP64 step's limited slope ratio: for i < n, out[i] = kc * superbee(a[i] /
+ * b[i]) as the FP64 kernels form it (the division above fused with the limiter; at b = +0 the
+ * division's limit), computed on the current device from host arrays; it equals kc times
+ * the reference's superbee (simple/le_core.c:38) of the correctly rounded quotient. */
+int le2d_selftest_limiter(const double *a, const double *b, double kc, long long n, double *out);
+
 /* ---- One grid over several devices (row slabs) ---------------------------------------
  * The reference's multi-GPU step (cuda5/cuda6 le_core.cu:374-509: one process, row slabs,
  * peer copies of the rows next to each cut).  The task's grid (its size, dt, h, material

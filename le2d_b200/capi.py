@@ -48,7 +48,7 @@ EXPORTS = [
     "le2d_server_stats", "le2d_now", "le2d_diagnostics_noalloc", "le2d_autotune", "le2d_autotune_reset",
     "le2d_batch_autotune", "le2d_batch_autotune_reset",
     "le2d_slabs_create", "le2d_slabs_destroy", "le2d_slabs_rows", "le2d_slabs_upload",
-    "le2d_slabs_download", "le2d_slabs_step_n", "le2d_slabs_wait", "le2d_selftest_ratio",
+    "le2d_slabs_download", "le2d_slabs_step_n", "le2d_slabs_wait", "le2d_selftest_ratio", "le2d_selftest_limiter",
     "le2d_rows_out", "le2d_rows_in", "le2d_check_violations",
 ]
 
@@ -198,6 +198,8 @@ class Lib:
         L.le2d_rows_in.argtypes = [P(self.le_task), ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.le2d_selftest_ratio.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
                                           ctypes.c_void_p, ctypes.c_void_p]
+        L.le2d_selftest_limiter.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_longlong,
+                                            ctypes.c_void_p]
         L.le2d_diagnostics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
                                                ctypes.c_longlong, R, R, R, R, R, ctypes.c_void_p,
                                                P(self.le2d_diag_t)]
@@ -315,6 +317,17 @@ class Lib:
         if rc:
             raise RuntimeError(self.strerror(rc))
         return fast, ieee
+
+    def selftest_limiter(self, a: np.ndarray, b: np.ndarray, kc: float) -> np.ndarray:
+        """kc * superbee(a / b) as the FP64 step kernels form it, on the device."""
+        a = np.ascontiguousarray(a, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        assert a.shape == b.shape and a.ndim == 1
+        out = np.empty_like(a)
+        rc = self.lib.le2d_selftest_limiter(a.ctypes.data, b.ctypes.data, kc, a.size, out.ctypes.data)
+        if rc:
+            raise RuntimeError(self.strerror(rc))
+        return out
 
     def sim_time(self, t):
         tt, st = ctypes.c_double(0.0), ctypes.c_longlong(0)

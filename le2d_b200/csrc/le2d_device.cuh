@@ -122,14 +122,16 @@ __device__ __forceinline__ float ratio(float a, float b) {
 // A select, not a branch: a branch per ratio costs more than the division.  The tie test
 // reads b's high word with an integer compare (zero for +0 and for nothing else in range),
 // which keeps it off the FP64 pipe the step is bound by.
-__device__ __forceinline__ double ratio(double a, double b) {
+__device__ __forceinline__ double quotient(double a, double b) {
   double y0;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(b));
   const double y = fma(y0, fma(-b, y0, 1.0), y0);
   const double q = a * y;
-  const double r = fma(fma(-b, q, a), y, q);
+  return fma(fma(-b, q, a), y, q);
+}
+__device__ __forceinline__ double ratio(double a, double b) {
   const double inf = __hiloint2double((__double2hiint(a) & (int)0x80000000) | 0x7ff00000, 0);
-  return __double2hiint(b) == 0 ? inf : r;
+  return __double2hiint(b) == 0 ? inf : quotient(a, b);
 }
 
 __device__ __forceinline__ float max3(float a, float b, float c) {
@@ -146,27 +148,31 @@ __device__ __forceinline__ double max3(double a, double b, double c) { return fm
 __device__ __forceinline__ float psi(float r, float kc) {
   return kc * fmaxf(__saturatef(r + r), fminf(2.0f, r));
 }
-// FP64 without floating-point compares: superbee(r) is one of 0, 2r, 1, r and 2, and which
-// one follows from r's high word h alone, because the breakpoints 0.5, 1 and 2 have zero low
-// words (so, for r >= 0, r < 1 <=> h < h(1), and so on): r in [1, 2) keeps r, below that 1,
-// from 2 on (with +inf) 2 -- a clamp of h to [h(1), h(2)] with the low word kept only
-// inside -- then 2r below 0.5 and 0 for r <= 0.  The FP64 ratio never returns NaN (a tie
-// gives copysign(inf, a), see ratio(double)); a positive NaN would land on 2 like the
-// reference's superbee(NaN).  The product kc * superbee(r), kc = (1 - k) / 2, rounds like
-// the reference's `limiter(r) / 2.0 * (1.0 - c)`: halving is exact.  The reference returns
-// -0 for r = -0 where this gives +0 (the same number).
-__device__ __forceinline__ double psi(double r, double kc) {
-  constexpr int kH05 = 0x3fe00000, kH1 = 0x3ff00000, kH2 = 0x40000000;  // high words of 0.5, 1, 2
-  const int h = __double2hiint(r), l = __double2loint(r);
-  const bool small = h < kH05, pos = h > 0;
+__device__ __forceinline__ float psi_ratio(float a, float b, float kc) { return psi(ratio(a, b), kc); }
+// FP64: kc * superbee(a / b), the limited slope ratio, without floating-point compares.
+// superbee(r) is one of 0, 2r, 1, r and 2, and which one follows from r's high word h alone,
+// because the breakpoints 0.5, 1 and 2 have zero low words (so, for r >= 0, r < 1 <=>
+// h < h(1), and so on).  Below 1, t = h + 2^20 (one more in the exponent field: 2r, r being a
+// normal number there -- the ratios' operands are at least 2^-73 or 0) capped at h(1) gives 2r
+// below 0.5 and 1 from 0.5 on; from 1 on, t = h capped at h(2) gives r below 2 and 2 from 2
+// on (with +inf); the low word stays only below the cap; r <= 0 (h <= 0 as a signed word,
+// -0 included) gives 0.  Integer operations keep the FP64 pipe, which bounds the step, free.
+// At a tie (b = +0) the division's limit, +-inf for a != 0 and NaN for 0 / 0 (superbee 2, 0
+// and 2), enters as the high word of a with the exponent bits set: negative for a < 0 (0),
+// at least h(2) otherwise (2) -- a is never -0.  The product kc * superbee(r), kc =
+// (1 - k) / 2, rounds like the reference's `limiter(r) / 2.0 * (1.0 - c)`: halving is exact.
+// The reference returns -0 for r = -0 where this gives +0 (the same number).
+// le2d_selftest_limiter compares it with kc times the reference's superbee of IEEE a / b.
+__device__ __forceinline__ double psi_ratio(double a, double b, double kc) {
+  constexpr int kH1 = 0x3ff00000, kH2 = 0x40000000;  // high words of 1 and 2
+  const double r = quotient(a, b);
+  const int h = __double2hiint(b) == 0 ? (__double2hiint(a) | 0x7ff00000) : __double2hiint(r);
+  const bool below1 = h < kH1, pos = h > 0;
+  const int t = below1 ? h + 0x00100000 : h;
+  const int cap = below1 ? kH1 : kH2;
   // written as selects: a branch here would diverge within the warp
-  int ho = min(max(h, kH1), kH2);
-  int lo = h >= kH1 && h < kH2 ? l : 0;
-  // 0 < r < 0.5: 2r, by one more in the exponent field (r is a normal number there: the
-  // ratios' operands are at least 2^-73 or 0); r <= 0: 0.  An integer add instead of a
-  // floating-point one keeps the FP64 pipe, which bounds the step, free.
-  ho = small ? (pos ? h + 0x00100000 : 0) : ho;
-  lo = small ? (pos ? l : 0) : lo;
+  const int ho = pos ? min(t, cap) : 0;
+  const int lo = pos && t < cap ? __double2loint(r) : 0;
   return kc * __hiloint2double(ho, lo);
 }
 

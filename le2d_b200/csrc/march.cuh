@@ -170,7 +170,7 @@ __device__ __forceinline__ void sweep_x_lane_exact(double (&f)[NF][V], const Swe
       for (int e = 0; e <= V; ++e) d[e] = ex::sub(w[k][e + 1], w[k][e]);
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        const double ps = psi(ratio(ex::add(d[v], eps), ex::add(d[v + 1], eps)), kc);
+        const double ps = psi_ratio(ex::add(d[v], eps), ex::add(d[v + 1], eps), kc);
         fl[v] = ex::add(w[k][v + 1], ex::mul(ps, d[v + 1]));
       }
       const double f_in = __shfl_up_sync(kAll, fl[V - 1], 1);
@@ -184,7 +184,7 @@ __device__ __forceinline__ void sweep_x_lane_exact(double (&f)[NF][V], const Swe
       for (int e = 0; e <= V; ++e) d[e] = ex::sub(w[k][e + 1], w[k][e]);
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        const double ps = psi(ratio(ex::sub(eps, d[v + 1]), ex::sub(eps, d[v])), kc);
+        const double ps = psi_ratio(ex::sub(eps, d[v + 1]), ex::sub(eps, d[v]), kc);
         gl[v] = ex::sub(w[k][v + 1], ex::mul(ps, d[v]));
       }
       const double g_in = __shfl_down_sync(kAll, gl[0], 1);
@@ -236,7 +236,7 @@ __device__ __forceinline__ void sweep_x_lane_diff(T (&f)[NF][V], const Sweep<T>&
       T ps[V], t[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        ps[v] = psi(ratio(d[k][v] + eps, d[k][v + 1] + eps), kc);
+        ps[v] = psi_ratio(d[k][v] + eps, d[k][v + 1] + eps, kc);
         t[v] = fma(ps[v], d[k][v + 1], -d[k][v + 1]);
       }
       const T t_in = __shfl_up_sync(kAll, t[V - 1], 1);
@@ -248,7 +248,7 @@ __device__ __forceinline__ void sweep_x_lane_diff(T (&f)[NF][V], const Sweep<T>&
       T ps[V], h[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        ps[v] = psi(ratio(eps - d[k][v + 1], eps - d[k][v]), kc);
+        ps[v] = psi_ratio(eps - d[k][v + 1], eps - d[k][v], kc);
         h[v] = fma(-ps[v], d[k][v], d[k][v]);
       }
       const T h_in = __shfl_down_sync(kAll, h[0], 1);
@@ -515,7 +515,7 @@ struct YPipe<double, V> {
         wr[q][v] = wp[2 * q];
         const double dd = ex::sub(wc[2 * q + 1], wp[2 * q + 1]);
         const double q1 = ex::sub(eps, dd);
-        const double ps = psi(ratio(q1, q2[q][v]), kc);
+        const double ps = psi_ratio(q1, q2[q][v], kc);
         const double g1 = ex::sub(wp[2 * q + 1], ex::mul(ps, d2[q][v]));
         dl[q][v] = ex::sub(g2[q][v], g1);
         g2[q][v] = g1;
@@ -547,7 +547,7 @@ struct YPipe<double, V> {
         const double kc = q ? cy.kc2 : cy.kc1;
         const double dd = dfw[q][v];
         const double p1 = ex::add(dd, eps);
-        const double ps = psi(ratio(p2[q][v], p1), kc);
+        const double ps = psi_ratio(p2[q][v], p1, kc);
         const double f1 = ex::add(wr[q][v], ex::mul(ps, dd));
         dr[q][v] = ex::sub(f1, f2[q][v]);
         f2[q][v] = f1;

@@ -109,3 +109,47 @@ def test_ratio_tie_neighbourhood(lib):
     b = np.concatenate([np.tile(p, p.size), np.tile(p, 61)])
     fast, ieee = lib.selftest_ratio(a, b)
     assert np.array_equal(fast, ieee)
+
+
+def _superbee_reference(r):
+    """The reference's superbee (simple/le_core.c:31-38) with its comparison macros:
+    le_max(0, le_max(le_min(1, 2r), le_min(2, r))), le_min(a, b) = a > b ? b : a and
+    le_max(a, b) = a > b ? a : b -- so superbee(NaN) = 2."""
+    with np.errstate(invalid="ignore", over="ignore"):
+        two = 2.0 * r
+        m1 = np.where(1.0 > two, two, 1.0)
+        m2 = np.where(2.0 > r, r, 2.0)
+        mx = np.where(m1 > m2, m1, m2)
+        return np.where(0.0 > mx, 0.0, mx)
+
+
+def test_limiter_matches_reference_superbee(lib):
+    """The FP64 step's limited slope ratio (psi_ratio: the division fused with the limiter,
+    which picks 0, 2r, 1, r or 2 from the quotient's high word) against kc times the
+    reference's superbee of the IEEE quotient, bit for bit: random and slope-form operand
+    pairs, quotients at and next to the breakpoints 0, 0.5, 1 and 2, and ties (b = +0)."""
+    rng = np.random.default_rng(77)
+    parts = [_random_pairs(rng, 300_000, -40, 40), _slope_pairs(rng, 300_000), _exact_quotients(rng, 100_000)]
+    b = np.ldexp(rng.uniform(1.0, 2.0, 4000), rng.integers(-60, 60, 4000))
+    for q in (0.5, 1.0, 2.0, 0.25, 4.0):
+        for k in (-2, -1, 0, 1, 2):  # the breakpoint and its neighbours a few ulps away
+            qq = q + k * np.spacing(q)
+            parts.append((b * qq, b))
+    parts.append((-b, b))
+    a = np.concatenate([p[0] for p in parts])
+    b = np.concatenate([p[1] for p in parts])
+    with np.errstate(over="ignore", under="ignore"):
+        q = np.abs(a / b)
+    ok = (np.isfinite(q) & ((q > 2.0 ** -900) | (q == 0.0)) & (q < 2.0 ** 1000) & (np.abs(b) >= 2.0 ** -900)
+          & (np.abs(a) < 2.0 ** 1000))
+    a, b = a[ok], b[ok]
+    ties = np.array([1.0, -1.0, 0.0, EPS, -EPS, 2.0 ** -73, -(2.0 ** -73), 3.0])
+    a = np.concatenate([a, ties])
+    b = np.concatenate([b, np.zeros_like(ties)])
+    for kc in (0.375, 0.25, (1.0 - 0.3) / 2.0):
+        got = lib.selftest_limiter(a, b, kc)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            want = kc * _superbee_reference(a / b)
+        bad = np.flatnonzero(got != want)
+        print(f"\n{a.size} operand pairs, kc={kc}: differing from the reference's limiter: {bad.size}")
+        assert bad.size == 0, [(a[i], b[i], got[i], want[i]) for i in bad[:8]]
