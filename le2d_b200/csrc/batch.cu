@@ -117,6 +117,17 @@ __device__ __forceinline__ bool launch_ending(const BatchCtl* ctl) {
   return *reinterpret_cast<const volatile int*>(&ctl->status) != 0;
 }
 
+// The one-step kernel's counterpart: the item's step constants in the warp's slot.
+template <typename T>
+__device__ __forceinline__ const StepConsts<T>& load_step_consts(StepConsts<T>* slot, const StepConsts<T>& c) {
+  constexpr int kw = (int)(sizeof(StepConsts<T>) / 4);
+  const unsigned* src = reinterpret_cast<const unsigned*>(&c);
+  unsigned* dst = reinterpret_cast<unsigned*>(slot);
+  for (int i = threadIdx.x & 31; i < kw; i += 32) dst[i] = src[i];
+  __syncwarp();
+  return *slot;
+}
+
 template <typename T, int V, int MINB>
 __global__ void __launch_bounds__(kWarps * 32, MINB)
     batch_kernel(const BatchInst<T>* __restrict__ insts, const BatchTile* __restrict__ tiles,
@@ -125,6 +136,9 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   T* ring = reinterpret_cast<T*>(smem_raw) + (threadIdx.x >> 5) * march::warp_smem_elems<T, V, kNpf>();
+  StepConsts<T>* cslot = reinterpret_cast<StepConsts<T>*>(
+                             smem_raw + kWarps * march::warp_smem_elems<T, V, kNpf>() * sizeof(T)) +
+                         (threadIdx.x >> 5);
   const long long total = step_items[nsteps];
   int r = 0;
   while (true) {
@@ -147,7 +161,8 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
     const long long step_after = I.abs_step0 + r + 1;  // absolute step count after this step
     if (I.trace != nullptr && step_after % I.trace_every == 0)
       tap = march::RowTap<T>{I.trace + (step_after / I.trace_every - 1) * 2 * I.pitch, I.trace_row};
-    march::march_tile<T, V, kNpf, true, true, false>(g, I.c, bt.strip, y0, y1, ring, tap);
+    march::march_tile<T, V, kNpf, true, true, false>(g, load_step_consts(cslot, I.c), bt.strip, y0, y1, ring,
+                                                     tap);
     __syncwarp();
     const int tile_id = I.tile_base + bt.seg * I.nstrips + bt.strip;
     if (lane == 0 && !(r == 0 && tile_id == stall_plus1 - 1)) {
@@ -291,18 +306,23 @@ __global__ void __launch_bounds__(kWarps * 32, MINB)
 template <typename T>
 struct BatchKernelOf;
 // FP32: two-step items on warp pairs (4 columns per lane, 168 registers: 12 warps per SM);
-// FP64: one-step items on single warps (2 columns per lane, 8 warps per SM).
+// FP64: one-step items on single warps (2 columns per lane, 8 warps per SM); each warp's
+// ring is followed, after all the block's rings, by its step-constants slot.
 template <>
 struct BatchKernelOf<float> {
   static constexpr int V = 4, MINB = 3, DEPTH = 2;
   static void* fn() { return (void*)batch_pair_kernel<float, V, MINB>; }
   static size_t smem() { return (size_t)(kWarps / 2) * batch_pair_bytes<float, V>(); }
 };
+static_assert(march::warp_smem_elems<double, 2, kNpf>() * sizeof(double) % alignof(StepConsts<double>) == 0,
+              "the step-constants slots after the rings must stay aligned");
 template <>
 struct BatchKernelOf<double> {
   static constexpr int V = 2, MINB = 2, DEPTH = 1;
   static void* fn() { return (void*)batch_kernel<double, V, MINB>; }
-  static size_t smem() { return (size_t)kWarps * march::warp_smem_elems<double, V, kNpf>() * sizeof(double); }
+  static size_t smem() {
+    return (size_t)kWarps * (march::warp_smem_elems<double, V, kNpf>() * sizeof(double) + sizeof(StepConsts<double>));
+  }
 };
 
 }  // namespace
