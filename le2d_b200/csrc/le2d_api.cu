@@ -106,10 +106,10 @@ long long row_pitch(int nx) { return le2d::row_pitch_elems(nx); }
 
 // Fused-kernel variant used for new tasks: LE2D_FUSED_VARIANT if set, else the fastest
 // measured on large grids (FP32: two steps per launch on producer / consumer warp pairs,
-// 4 columns per lane, 16 warps per SM, one pair per block, interior tiles first and on the
-// lean loops; FP64: one step per launch, 2 columns per lane, interior tiles first and on
-// the lean one-step loop in 128 registers, 16 warps per SM -- the FP64 two-step variants
-// measured slower).
+// 4 columns per lane, 16 warps per SM, one pair per block, boundary tiles first, interior
+// tiles on the lean loops; FP64: one step per launch, 2 columns per lane, boundary tiles
+// first, interior tiles on the lean one-step loop in 128 registers, 16 warps per SM -- the
+// FP64 two-step variants measured slower).
 int default_variant() {
   static int v = -2;
   if (v == -2) {

@@ -42,12 +42,19 @@ __device__ __forceinline__ void segment_rows(const FusedParams<T>& p, int seg, i
   }
 }
 
-// Tile of a task when the interior tiles come first (in segment-major order) and the
-// boundary tiles -- the segments above g_lo and from g_hi on, and the strips outside
-// [s_lo, s_hi) of the segments between -- after them.
+// Tile of a task when the boundary tiles -- the segments above g_lo and from g_hi on, and
+// the strips outside [s_lo, s_hi) of the segments between -- come first and the interior
+// tiles (in segment-major order) after them.  The boundary tiles take the general loops,
+// which are slower per tile than the lean ones: dealt out first, they finish while interior
+// tiles still fill the device, and the launch ends on lean tiles.  Measured with the interior
+// tiles first instead (the tail of every launch then being boundary tiles on a thinning
+// device): 3-9 % slower (8192^2: 177.0 against 181.7 Gnu/s; 4096^2: 146.0 against 155.0;
+// 2048 x 8192: 142.0 against 154.3).
 template <typename T>
-__device__ __forceinline__ void interior_first(const FusedParams<T>& p, int task, int& strip, int& seg) {
+__device__ __forceinline__ void boundary_first(const FusedParams<T>& p, int task, int& strip, int& seg) {
   const int ni = p.s_hi - p.s_lo, ng = p.g_hi - p.g_lo;
+  const int nb = p.ntasks - ni * ng;  // boundary tiles
+  task = task < nb ? ni * ng + task : task - nb;
   if (task < ni * ng) {
     seg = p.g_lo + task / ni;
     strip = p.s_lo + task % ni;
@@ -93,7 +100,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) fused_step_kernel(const Fus
   T* smem = reinterpret_cast<T*>(smem_raw) + wib * warp_elems<T, V, NPF, D>();
   int strip = task % p.nstrips;
   int seg = task / p.nstrips;
-  if constexpr (F == 2) interior_first(p, task, strip, seg);
+  if constexpr (F == 2) boundary_first(p, task, strip, seg);
   int y0, y1;
   segment_rows(p, seg, y0, y1);
   if constexpr (D == 1 && F >= 1) {  // interior tiles on the lean loop
@@ -130,7 +137,7 @@ __global__ void __launch_bounds__(W * 32, MINB) fused_pair_kernel(const FusedPar
   if (task == p.pair.stall_task && producer) return;  // test hook
   int strip = task % p.nstrips;
   int seg = task / p.nstrips;
-  if constexpr (F == 2) interior_first(p, task, strip, seg);
+  if constexpr (F == 2) boundary_first(p, task, strip, seg);
   int y0, y1;
   segment_rows(p, seg, y0, y1);
   T* smem = reinterpret_cast<T*>(base);
@@ -161,8 +168,8 @@ __global__ void __launch_bounds__(W * 32, MINB) fused_pair_kernel(const FusedPar
 // shared-memory input ring (NPF - 1 rows are in flight ahead of the row being swept),
 // the temporal-block depth D (steps per launch), P = 1 for two-step tiles on warp pairs,
 // warps per block W, and F: 1 = interior tiles on the lean loops, 2 = the same with the
-// interior tiles dealt out first (so the general loops, which boundary tiles take, run
-// beside the lean ones on an SM only at the end of the launch).
+// boundary tiles dealt out first (boundary_first: the general loops they take run beside
+// the lean ones on an SM only at the start of the launch, which ends on lean tiles).
 template <typename T, int VAR>
 struct VariantCfg;
 template <> struct VariantCfg<float, 0> { static constexpr int V = 4, MINB = 3, NPF = 2, D = 1, P = 0, W = 4, F = 0; };
@@ -331,36 +338,44 @@ constexpr int kWaves = 8;
 
 // The segment length L that minimises a model of the launch time fitted to measured
 // launches,
-//   time ~ (w + beta + alpha (ceil(w) - w)) (L + h),   w = tiles / resident tiles,
+//   time ~ (w + beta + alpha (ceil(w) - w)) (L + h) (1 + kappa L / 128),   w = tiles / resident tiles,
 // w being the launch's waves of tiles, L + h the rows of a tile's march (h for its halo rows
-// and the fill of its pipeline) and the idle part of the last wave charged at alpha.  Fits:
-//   warp-pair (two-step) variants, the FP32 default measured on grids 1024^2 to 16384^2,
-//   8192 x 2048 and 2048 x 8192 with segments of 32 to 256 rows: h = 6, beta = 0.2,
-//   alpha = 0.3 -- within 2 % of the fastest measured length on each of those grids but
-//   8192 x 2048 (3 %), where the 8-wave rule lost up to 6 % (158 against 168 Gnu/s on
-//   6000^2, 173 against 177 on 8192^2);
+// and the fill of its pipeline), alpha the charge for the idle part of the last wave and
+// kappa one for long tiles (the tiles resident at a time then span more rows of the grid).
+// L is one of the lengths the fit measured.  Fits:
+//   warp-pair (two-step) variants, the FP32 default with its boundary tiles dealt out first,
+//   measured on 2048^2 to 16384^2, 8192 x 2048 and 2048 x 8192 with segments of 32 to 256
+//   rows: h = 10, beta = 0.1, alpha = 0.5, kappa = 0.02 -- the fastest measured length on
+//   each of those grids (an earlier fit without the length term: up to 7 % below it, e.g.
+//   147.4 against 158.3 Gnu/s on 3000^2, 155.1 against 158.4 on 4096^2; the earlier rule of
+//   about 8 waves of tiles: up to 13 % below it);
 //   FP64 one-step variants, the FP64 default measured on 2048^2 to 12000^2 with segments of
-//   16 to 128 rows: h = 2, beta = 0.1, alpha = 0.3 -- 42.5 against 40.3 Gnu/s on 2048^2,
-//   49.3 against 46.6 on 4096^2 under the 8-wave rule.
-// Lengths above 256 rows were not measured and are not considered.
+//   16 to 128 rows: h = 2, beta = 0.1, alpha = 0.3, kappa = 0 -- within 3 % of the fastest
+//   measured length (42.5 against 40.3 Gnu/s on 2048^2, 49.3 against 46.6 on 4096^2 under the
+//   8-wave rule).
 struct SegModel {
-  double h, beta, alpha;
-  int step;
+  double h, beta, alpha, kappa;
+  const int* lens;
+  int nlens;
 };
-constexpr SegModel kPairModel{6.0, 0.2, 0.3, 16};
-constexpr SegModel kStepModelF64{2.0, 0.1, 0.3, 8};
+constexpr int kPairLens[] = {32, 48, 64, 80, 96, 128, 160, 192, 256};
+constexpr int kStepLensF64[] = {16, 24, 32, 40, 48, 56, 64, 80, 96, 112, 128};
+constexpr SegModel kPairModel{10.0, 0.1, 0.5, 0.02, kPairLens, 9};
+constexpr SegModel kStepModelF64{2.0, 0.1, 0.3, 0.0, kStepLensF64, 11};
 
 inline int model_segment(const SegModel& m, int ny, int nstrips, int resident_tiles, int min_len) {
-  int best_len = min_len;
+  int best_len = min_len < ny ? min_len : ny;
   double best = 1e300;
-  for (int len = min_len; len <= 256 && len < ny + m.step; len += m.step) {
-    const int l = len < ny ? len : ny;
+  for (int i = 0; i < m.nlens; ++i) {
+    if (m.lens[i] < min_len) continue;
+    const int l = m.lens[i] < ny ? m.lens[i] : ny;
     const double w = (double)nstrips * ((ny + l - 1) / l) / resident_tiles;
-    const double t = (w + m.beta + m.alpha * (std::ceil(w) - w)) * (l + m.h);
+    const double t = (w + m.beta + m.alpha * (std::ceil(w) - w)) * (l + m.h) * (1.0 + m.kappa * l / 128.0);
     if (t < best) {
       best = t;
       best_len = l;
     }
+    if (l == ny) break;
   }
   return best_len;
 }
