@@ -349,10 +349,10 @@ constexpr int kWaves = 8;
 //   each of those grids (an earlier fit without the length term: up to 7 % below it, e.g.
 //   147.4 against 158.3 Gnu/s on 3000^2, 155.1 against 158.4 on 4096^2; the earlier rule of
 //   about 8 waves of tiles: up to 13 % below it);
-//   FP64 one-step variants, the FP64 default measured on 2048^2 to 12000^2 with segments of
-//   16 to 128 rows: h = 2, beta = 0.1, alpha = 0.3, kappa = 0 -- within 3 % of the fastest
-//   measured length (42.5 against 40.3 Gnu/s on 2048^2, 49.3 against 46.6 on 4096^2 under the
-//   8-wave rule).
+//   FP64 one-step variants, the FP64 default measured on 2048^2 to 12000^2 and 8192 x 2048
+//   with segments of 16 to 128 rows: h = 8, beta = 0.3, alpha = 0, kappa = 0.1 -- within 1 %
+//   of the fastest measured length on each (the 8-wave rule: up to 10 % below it, e.g. 40.3
+//   against 44.2 Gnu/s on 2048^2, 46.6 against 51.3 on 4096^2).
 struct SegModel {
   double h, beta, alpha, kappa;
   const int* lens;
@@ -361,7 +361,7 @@ struct SegModel {
 constexpr int kPairLens[] = {32, 48, 64, 80, 96, 128, 160, 192, 256};
 constexpr int kStepLensF64[] = {16, 24, 32, 40, 48, 56, 64, 80, 96, 112, 128};
 constexpr SegModel kPairModel{10.0, 0.1, 0.5, 0.02, kPairLens, 9};
-constexpr SegModel kStepModelF64{2.0, 0.1, 0.3, 0.0, kStepLensF64, 11};
+constexpr SegModel kStepModelF64{8.0, 0.3, 0.0, 0.1, kStepLensF64, 11};
 
 inline int model_segment(const SegModel& m, int ny, int nstrips, int resident_tiles, int min_len) {
   int best_len = min_len < ny ? min_len : ny;
