@@ -65,13 +65,126 @@ struct DevTask {
   // CUDA graph of kGraphSteps steps starting from buffer graph_cur.
   cudaGraphExec_t graph = nullptr;
   int graph_cur = -1, graph_method = -1, graph_far_rot = -1;
+  bool graph_halves = false;
   StepConsts<T> graph_consts;
+  // Fused launches in halves (halves_launch): hs[0] the band of rows around the middle of
+  // the grid (high priority), hs[1] / hs[2] the rows above / below it; hev[i][k & 1] after
+  // stream i's part of launch k of the current sequence, hk launches so far.
+  bool halves = false;
+  cudaStream_t hs[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t hev[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+  cudaEvent_t fork_ev = nullptr;
+  long long hk = 0;
 };
 
 constexpr int kGraphSteps = 64;  // even, so a replay leaves the current buffer unchanged
 // Bound of every wait between the two warps of a warp-pair tile (they share a block, so a
 // wait that long means a fault in the kernel, not a slow partner).
 constexpr unsigned long long kPairWaitNs = 1000000000ull;
+
+// Fused launches in halves.  One launch over the whole grid ends on a partly idle device:
+// its last wave of tiles thins out before the next launch, which depends on all of it,
+// starts.  Cut in three -- the band of kBand rows on each side of the middle row, the rows
+// above it and the rows below it -- a launch's parts depend on the previous launch's only
+// where their stencils meet: each interior part on the previous band (which it reads, and
+// whose reads of its rows it must not overtake), the band on both previous interior parts.
+// So the upper and lower parts run on streams of their own and overlap each other's ends,
+// as the row slabs of two devices do (slabs.cu), without copies: the parts share the
+// task's buffers and write disjoint rows.  The stencil of a launch reaches 4 rows (two
+// steps of two), so kBand = 4.  Bitwise the same results as whole launches.
+constexpr int kBand = 4;
+constexpr int kMinHalvesRows = 256;  // grids with fewer rows launch whole
+
+// Whether a task's fused launches go in halves.  Measured (Gnu/s, whole / halves): FP32 two-step
+// plans on 8192^2 181.5 / 191.8, 16384^2 192.4 / 195.7, 1024^2 47.3 / 51.2, but on grids whose
+// launch is about one wave of tiles (2048^2, 3000^2, 4096^2, 8192 x 2048, 2048 x 8192: 0.93 to
+// 0.99 waves) 0 to 2 % slower -- a launch that fits in one wave leaves no end to overlap;
+// FP64 one-step plans on 2048^2 44.6 / 46.1, 4096^2 51.1 / 53.7, 8192^2 55.9 / 57.2.  So:
+// on grids of at least kMinHalvesRows rows, except two-step plans of 0.5 to 1.5 waves.
+// LE2D_HALVES=1 / 0 overrides it (on every grid of at least 4 kBand rows / never).
+bool halves_for(int ny, const FusedPlan& p, int resident_warps) {
+  static int mode = -2;
+  if (mode == -2) {
+    const char* e = getenv("LE2D_HALVES");
+    mode = e ? (atoi(e) != 0 ? 1 : 0) : -1;
+  }
+  if (mode == 0 || ny < 4 * kBand) return false;
+  if (mode == 1) return true;
+  if (ny < kMinHalvesRows) return false;
+  if (p.depth == 2 && resident_warps > 0) {
+    const double waves = (double)p.ntasks * p.warps_per_task / resident_warps;
+    if (waves > 0.5 && waves < 1.5) return false;
+  }
+  return true;
+}
+
+cudaError_t create_halves(DevTask* d) {
+  int lo = 0, hi = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&d->hs[0], cudaStreamNonBlocking, hi);
+  for (int i = 1; i < 3 && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&d->hs[i], cudaStreamNonBlocking);
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i)
+    for (int j = 0; j < 2 && e == cudaSuccess; ++j) e = cudaEventCreateWithFlags(&d->hev[i][j], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d->fork_ev, cudaEventDisableTiming);
+  return e;
+}
+
+void destroy_halves(DevTask* d) {
+  for (int i = 0; i < 3; ++i) {
+    if (d->hs[i]) {
+      cudaStreamSynchronize(d->hs[i]);
+      cudaStreamDestroy(d->hs[i]);
+    }
+    for (int j = 0; j < 2; ++j)
+      if (d->hev[i][j]) cudaEventDestroy(d->hev[i][j]);
+  }
+  if (d->fork_ev) cudaEventDestroy(d->fork_ev);
+}
+
+// Starts a sequence of launches in halves: the three streams wait for the task's stream.
+cudaError_t halves_begin(DevTask* d) {
+  d->hk = 0;
+  cudaError_t e = cudaEventRecord(d->fork_ev, d->stream);
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(d->hs[i], d->fork_ev, 0);
+  return e;
+}
+
+// Ends it: the task's stream waits for the three streams.
+cudaError_t halves_end(DevTask* d) {
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+    cudaEvent_t ev = d->hev[i][d->hk & 1];
+    e = cudaEventRecord(ev, d->hs[i]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(d->stream, ev, 0);
+  }
+  return e;
+}
+
+// Launch k of the sequence, from a into b, in three parts.
+cudaError_t halves_launch(DevTask* d, const T* a, T* b, const StepConsts<T>& c, const FusedPlan& pl,
+                          const le2d::PairCtl& pc) {
+  const long long k = d->hk;
+  const int mid = d->ny / 2;
+  const int lo[3] = {mid - kBand, 0, mid + kBand}, hi[3] = {mid + kBand, mid - kBand, d->ny};
+  cudaError_t e = cudaSuccess;
+  if (k > 0) {  // the band after both interior parts of launch k-1
+    e = cudaStreamWaitEvent(d->hs[0], d->hev[1][(k + 1) & 1], 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(d->hs[0], d->hev[2][(k + 1) & 1], 0);
+  }
+  if (e == cudaSuccess)
+    e = le2d::launch_fused_rows<T>(a, b, d->nx, d->ny, d->pitch, d->plane, c, 0, pl, pc, 2 * kBand, 1, &lo[0],
+                                   &hi[0], d->hs[0]);
+  if (e == cudaSuccess) e = cudaEventRecord(d->hev[0][k & 1], d->hs[0]);
+  for (int i = 1; i < 3 && e == cudaSuccess; ++i) {  // each interior part after the band of launch k-1
+    if (k > 0) e = cudaStreamWaitEvent(d->hs[i], d->hev[0][(k + 1) & 1], 0);
+    if (e == cudaSuccess)
+      e = le2d::launch_fused_rows<T>(a, b, d->nx, d->ny, d->pitch, d->plane, c, 0, pl, pc, pl.seg_len, 1, &lo[i],
+                                     &hi[i], d->hs[i]);
+    if (e == cudaSuccess) e = cudaEventRecord(d->hev[i][k & 1], d->hs[i]);
+  }
+  ++d->hk;
+  return e;
+}
 
 std::mutex g_mu;
 std::unordered_map<const void*, DevTask*> g_tasks;
@@ -136,6 +249,7 @@ void replan(DevTask* d, int variant, int seg_len) {
   }
   d->plan = p;
   d->plan1 = p;
+  d->halves = d->hs[0] != nullptr && halves_for(d->ny, p, resident);
   if (p.depth != 1) {  // odd remainders and le_step_soa run single steps
     const int v = sizeof(T) == 4 ? 2 : 15;  // the fastest one-step variant
     d->plan1 = le2d::plan_fused<T>(d->nx, d->ny, v, le2d::fused_resident_warps<T>(dev, v), kMinSeg);
@@ -165,7 +279,7 @@ std::pair<int, int> size_class(int nx, int ny) { return {ceil_log2(nx), ceil_log
 
 void release(DevTask* d);
 cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int method, int* cur,
-                       int max_steps, int* done);
+                       int max_steps, int* done, bool halves = false);
 
 // Times every variant x segment length on a scratch nx x ny state (a disk of radius
 // min(nx,ny)/4 on a zero field, c1 = 2, c2 = 1, rho = 1, Courant number 0.5).
@@ -322,11 +436,12 @@ int ensure_host_current(DevTask* d, le_task* task) {
 }
 
 // Queues one launch of at most max_steps (>= 1) steps from buf[cur] and adds the steps it
-// makes to *done.  The fused kernel writes buf[cur^1] and flips cur -- two steps when the
+// makes to *done (halves: a fused launch on clamped ends goes in halves, inside a sequence
+// that halves_begin opened).  The fused kernel writes buf[cur^1] and flips cur -- two steps when the
 // plan has temporal-block depth 2 and two are wanted (clamped ends only), else one; the
 // split scheme sweeps x into buf[cur^1] and y back into buf[cur].
 cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int method, int* cur,
-                       int max_steps, int* done) {
+                       int max_steps, int* done, bool halves) {
   T* a = d->buf[*cur];
   T* b = d->buf[*cur ^ 1];
   if (method == LE2D_METHOD_SPLIT) {
@@ -344,8 +459,10 @@ cudaError_t queue_step(DevTask* d, const StepConsts<T>& c, int far_rot, int meth
   pc.status = d->d_status;
   pc.wait_ns = kPairWaitNs;
   pc.stall_task = d->stall_pair;
-  cudaError_t e = le2d::launch_fused_step<T>(a, b, d->nx, d->ny, d->pitch, d->plane, c, far_rot,
-                                             pl, pc, d->stream);
+  cudaError_t e = halves && !far_rot
+                      ? halves_launch(d, a, b, c, pl, pc)
+                      : le2d::launch_fused_step<T>(a, b, d->nx, d->ny, d->pitch, d->plane, c, far_rot, pl, pc,
+                                                   d->stream);
   *cur ^= 1;
   *done += pl.depth;
   return e;
@@ -409,11 +526,14 @@ int run_steps(le_task* task, int nsteps, bool soa_entry, float* ms) {
     if (e != cudaSuccess) return record(d, LE2D_ECUDA, "event record", e);
   }
   int left = nsteps;
+  // fused launches on clamped ends in halves (halves_launch) on grids tall enough
+  const bool halves = d->halves && d->method == LE2D_METHOD_FUSED && !far_rot;
   // Long runs replay a captured graph of kGraphSteps steps (even count: buffers end where
   // they started).
   while (left >= kGraphSteps) {
     const bool valid = d->graph && d->graph_cur == d->cur && d->graph_method == d->method &&
-                       d->graph_far_rot == far_rot && same_consts(d->graph_consts, c);
+                       d->graph_far_rot == far_rot && d->graph_halves == halves &&
+                       same_consts(d->graph_consts, c);
     if (!valid) {
       if (d->graph) cudaGraphExecDestroy(d->graph);
       d->graph = nullptr;
@@ -421,8 +541,10 @@ int run_steps(le_task* task, int nsteps, bool soa_entry, float* ms) {
       e = cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal);
       if (e != cudaSuccess) return record(d, LE2D_ECUDA, "graph capture", e);
       int cur = d->cur;
+      if (halves) e = halves_begin(d);
       for (int s = 0; s < kGraphSteps && e == cudaSuccess;)
-        e = queue_step(d, c, far_rot, d->method, &cur, kGraphSteps - s, &s);
+        e = queue_step(d, c, far_rot, d->method, &cur, kGraphSteps - s, &s, halves);
+      if (halves && e == cudaSuccess) e = halves_end(d);
       cudaError_t e2 = cudaStreamEndCapture(d->stream, &g);
       if (e != cudaSuccess || e2 != cudaSuccess)
         return record(d, LE2D_ECUDA, "graph capture", e != cudaSuccess ? e : e2);
@@ -432,17 +554,26 @@ int run_steps(le_task* task, int nsteps, bool soa_entry, float* ms) {
       d->graph_cur = d->cur;
       d->graph_method = d->method;
       d->graph_far_rot = far_rot;
+      d->graph_halves = halves;
       d->graph_consts = c;
     }
     e = cudaGraphLaunch(d->graph, d->stream);
     if (e != cudaSuccess) return record(d, LE2D_ECUDA, "graph launch", e);
     left -= kGraphSteps;
   }
+  if (left > 0 && halves) {
+    e = halves_begin(d);
+    if (e != cudaSuccess) return record(d, LE2D_ECUDA, "step kernel launch", e);
+  }
   while (left > 0) {
     int done = 0;
-    e = queue_step(d, c, far_rot, d->method, &d->cur, left, &done);
+    e = queue_step(d, c, far_rot, d->method, &d->cur, left, &done, halves);
     if (e != cudaSuccess) return record(d, LE2D_ECUDA, "step kernel launch", e);
     left -= done;
+    if (left == 0 && halves) {
+      e = halves_end(d);
+      if (e != cudaSuccess) return record(d, LE2D_ECUDA, "step kernel launch", e);
+    }
   }
   if (ms) {
     e = cudaEventRecord(d->ev[1], d->stream);
@@ -461,6 +592,7 @@ int run_steps(le_task* task, int nsteps, bool soa_entry, float* ms) {
 
 void release(DevTask* d) {
   if (d->graph) cudaGraphExecDestroy(d->graph);
+  destroy_halves(d);
   if (d->ev[0]) cudaEventDestroy(d->ev[0]);
   if (d->ev[1]) cudaEventDestroy(d->ev[1]);
   if (d->stream) {
@@ -591,6 +723,7 @@ void le_init_task(le_task* task, const real dt, const le_vec2 h, const le_materi
       if (e == cudaSuccess) e = cudaEventCreate(&d->ev[0]);
       if (e == cudaSuccess) e = cudaEventCreate(&d->ev[1]);
       if (e == cudaSuccess) e = cudaMalloc(&d->d_diag, 16 * sizeof(double));
+      if (e == cudaSuccess) e = create_halves(d);
       if (e == cudaSuccess) e = cudaMalloc(&d->d_status, sizeof(int));
       if (e == cudaSuccess) e = cudaMemsetAsync(d->d_status, 0, sizeof(int), d->stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(d->mem, 0, dbytes, d->stream);
