@@ -234,7 +234,7 @@ def measure_ours(lib, prec, p, steps, warmup, dist, backend, device):
         dist_barrier(dist)
         e2e_slow = dist_max(dist, e2e_s, backend)
         assert np.isfinite(host_out2 if steps > 1 else host_out).all()
-        return slow_ms, clocks, e2e_slow, e2e_serial, ic, lib.get_plan(t)
+        return slow_ms, clocks, e2e_slow, e2e_serial, ic, {**lib.get_plan(t), "launch_parts": lib.launch_parts(t)}
     finally:
         lib.le_free_task(t)
         lib.le_free_task(e2e_t)
@@ -925,9 +925,12 @@ def main():
                                                                 backend, local)
     nu = p.node_updates * args.steps * world
     value = nu / (slow_ms * 1e-3)
-    depth = plan["depth"]  # time steps per fused-kernel launch (temporal blocking)
+    depth = plan["depth"]  # time steps per fused launch of the grid (temporal blocking)
     per_solve = p.steps // depth + p.steps % depth
-    launches = args.steps * per_solve
+    launches = args.steps * per_solve  # fused launches of the whole grid
+    # a launch of the grid in halves is 3 kernel launches (band, upper and lower rows) that
+    # overlap; its duration is that of the whole update
+    parts = plan.get("launch_parts", 1)
     avg_launch_s = slow_ms * 1e-3 / launches
     # algorithmic bytes: one read + one write of the state per node-update, depth node-updates
     # per node and launch
@@ -945,7 +948,7 @@ def main():
                      "peak_kind": peak_kind,
                      "traffic": traffic.get("bytes_per_launch") if traffic else None,
                      "kernel": kname, "variant": plan["variant"], "seg_len": plan["seg_len"],
-                     "algorithmic_bytes_per_launch": alg_bytes},
+                     "launch_parts": parts, "algorithmic_bytes_per_launch": alg_bytes},
         "e2e": {"value": nu / e2e_serial, "unit": "node-updates/s",
                 "h2d_bytes_per_step": int(ic.nbytes), "d2h_bytes_per_step": int(ic.nbytes),
                 "how": "one task: upload, steps and read-back of each solve in turn",
@@ -953,7 +956,7 @@ def main():
                 "pipelined_how": "two tasks alternate: solve k's upload and steps are queued before solve "
                                  "k-1's fields are read back, so copies (and the launch tails of the two "
                                  "streams) overlap"},
-        "gpu_launches": launches,  # fused-kernel launches in the timed region
+        "gpu_launches": launches * parts,  # step-kernel launches in the timed region
         "clocks": clocks,
     }
     if not args.no_fp64:
@@ -971,7 +974,8 @@ def main():
                         "roofline": {"bound": "hbm", "achieved": d_ach, "peak": peak, "unit": "GB/s",
                                      "frac": d_ach / peak,
                                      "kernel": (f"{'fused_pair_kernel' if d_plan['warps_per_task'] == 2 else 'fused_step_kernel'}"
-                                                f"<double, V={d_plan['lanes']}, depth={d_depth}>")},
+                                                f"<double, V={d_plan['lanes']}, depth={d_depth}>"),
+                                     "launch_parts": d_plan.get("launch_parts", 1)},
                         "clocks": d_clk}
     if world == 1 and not args.no_extras:
         # the batched and serving targets on the same GPU (one process; skipped under torchrun)

@@ -77,6 +77,12 @@ int le2d_set_variant(le_task *task, int variant, int seg_len);
 /* out[8] = {variant, columns per lane, segment rows, strips, tiles, blocks,
  * temporal-block depth, warps per tile (2: producer / consumer warp pair)}. */
 int le2d_get_plan(const le_task *task, int *out);
+/* *parts = kernel launches per fused launch of the grid: 1, or 3 when the task's launches go
+ * in halves (the band of rows around the middle row on a high-priority stream and the rows
+ * above and below it on two more streams, waiting for each other only where their stencils
+ * meet -- chosen per grid and plan where it measured faster; LE2D_HALVES=1 / 0 forces it on
+ * / off for tasks created afterwards). */
+int le2d_launch_parts(const le_task *task, int *parts);
 
 /* Autotuner: times every compiled fused-kernel variant (columns per lane, register bound,
  * input-ring depth, temporal-block depth, warp pair) and row-segment length on a scratch

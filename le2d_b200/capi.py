@@ -48,7 +48,7 @@ EXPORTS = [
     "le2d_server_stats", "le2d_now", "le2d_diagnostics_noalloc", "le2d_autotune", "le2d_autotune_reset",
     "le2d_batch_autotune", "le2d_batch_autotune_reset",
     "le2d_slabs_create", "le2d_slabs_destroy", "le2d_slabs_rows", "le2d_slabs_upload",
-    "le2d_slabs_download", "le2d_slabs_step_n", "le2d_slabs_wait", "le2d_selftest_ratio", "le2d_selftest_limiter",
+    "le2d_slabs_download", "le2d_slabs_step_n", "le2d_slabs_wait", "le2d_selftest_ratio", "le2d_selftest_limiter", "le2d_launch_parts",
     "le2d_rows_out", "le2d_rows_in", "le2d_check_violations",
 ]
 
@@ -198,6 +198,7 @@ class Lib:
         L.le2d_rows_in.argtypes = [P(self.le_task), ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.le2d_selftest_ratio.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
                                           ctypes.c_void_p, ctypes.c_void_p]
+        L.le2d_launch_parts.argtypes = [P(self.le_task), P(ctypes.c_int)]
         L.le2d_selftest_limiter.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_longlong,
                                             ctypes.c_void_p]
         L.le2d_diagnostics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
@@ -275,6 +276,14 @@ class Lib:
         return self.lib.le2d_set_variant(ctypes.byref(t), variant, seg_len)
 
     PLAN_KEYS = ("variant", "lanes", "seg_len", "nstrips", "ntasks", "blocks", "depth", "warps_per_task")
+
+    def launch_parts(self, t) -> int:
+        """Kernel launches per fused launch of the grid (3 when the task launches in halves)."""
+        v = ctypes.c_int(0)
+        rc = self.lib.le2d_launch_parts(ctypes.byref(t), ctypes.byref(v))
+        if rc:
+            raise RuntimeError(self.strerror(rc))
+        return v.value
 
     def get_plan(self, t) -> dict:
         out = (ctypes.c_int * len(self.PLAN_KEYS))()

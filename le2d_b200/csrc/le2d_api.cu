@@ -1002,6 +1002,14 @@ int le2d_get_plan(const le_task* task, int* out) {
   return LE2D_OK;
 }
 
+int le2d_launch_parts(const le_task* task, int* parts) {
+  DevTask* d = lookup(task);
+  if (!d) return LE2D_ENOTASK;
+  if (!parts) return LE2D_EINVAL;
+  *parts = d->halves ? 3 : 1;
+  return LE2D_OK;
+}
+
 int le2d_sim_time(const le_task* task, double* t, long long* steps) {
   DevTask* d = lookup(task);
   if (!d) return LE2D_ENOTASK;
