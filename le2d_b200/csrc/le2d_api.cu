@@ -95,27 +95,21 @@ constexpr unsigned long long kPairWaitNs = 1000000000ull;
 constexpr int kBand = 4;
 constexpr int kMinHalvesRows = 256;  // grids with fewer rows launch whole
 
-// Whether a task's fused launches go in halves.  Measured (Gnu/s, whole / halves): FP32 two-step
-// plans on 8192^2 181.5 / 191.8, 16384^2 192.4 / 195.7, 1024^2 47.3 / 51.2, but on grids whose
-// launch is about one wave of tiles (2048^2, 3000^2, 4096^2, 8192 x 2048, 2048 x 8192: 0.93 to
-// 0.99 waves) 0 to 2 % slower -- a launch that fits in one wave leaves no end to overlap;
-// FP64 one-step plans on 2048^2 44.6 / 46.1, 4096^2 51.1 / 53.7, 8192^2 55.9 / 57.2.  So:
-// on grids of at least kMinHalvesRows rows, except two-step plans of 0.5 to 1.5 waves.
-// LE2D_HALVES=1 / 0 overrides it (on every grid of at least 4 kBand rows / never).
-bool halves_for(int ny, const FusedPlan& p, int resident_warps) {
+// Whether a task's fused launches go in halves: on grids of at least kMinHalvesRows rows.
+// Measured (Gnu/s, best whole launch / halves, each at its fitted segment length): FP32
+// 1024^2 47.3 / 50.9, 3000^2 159.0 / 161.3, 4096^2 158.5 / 176.2, 6000^2 176.5 / 191.8,
+// 8192^2 181.8 / 195.2, 16384^2 192.7 / 197.2, 8192 x 2048 158.7 / 179.5, 2048 x 8192 158.3 /
+// 167.7, 2048^2 131.1 / 128.7; FP64 (whole segment lengths) 2048^2 44.6 / 46.1, 4096^2 51.1 /
+// 53.7, 8192^2 55.9 / 57.2.  LE2D_HALVES=1 / 0 overrides it (on every grid of at least
+// 4 kBand rows / never).
+bool halves_for(int ny) {
   static int mode = -2;
   if (mode == -2) {
     const char* e = getenv("LE2D_HALVES");
     mode = e ? (atoi(e) != 0 ? 1 : 0) : -1;
   }
   if (mode == 0 || ny < 4 * kBand) return false;
-  if (mode == 1) return true;
-  if (ny < kMinHalvesRows) return false;
-  if (p.depth == 2 && resident_warps > 0) {
-    const double waves = (double)p.ntasks * p.warps_per_task / resident_warps;
-    if (waves > 0.5 && waves < 1.5) return false;
-  }
-  return true;
+  return mode == 1 || ny >= kMinHalvesRows;
 }
 
 cudaError_t create_halves(DevTask* d) {
@@ -239,7 +233,8 @@ void replan(DevTask* d, int variant, int seg_len) {
   int dev = 0;
   cudaGetDevice(&dev);
   const int resident = le2d::fused_resident_warps<T>(dev, variant);
-  le2d::FusedPlan p = le2d::plan_fused<T>(d->nx, d->ny, variant, resident, kMinSeg);
+  d->halves = d->hs[0] != nullptr && halves_for(d->ny);
+  le2d::FusedPlan p = le2d::plan_fused<T>(d->nx, d->ny, variant, resident, kMinSeg, d->halves);
   if (seg_len > 0) {  // explicit segment length (tuning)
     const int wpb = p.threads / 32 / p.warps_per_task;  // tiles per block
     p.seg_len = seg_len < d->ny ? seg_len : d->ny;
@@ -249,7 +244,6 @@ void replan(DevTask* d, int variant, int seg_len) {
   }
   d->plan = p;
   d->plan1 = p;
-  d->halves = d->hs[0] != nullptr && halves_for(d->ny, p, resident);
   if (p.depth != 1) {  // odd remainders and le_step_soa run single steps
     const int v = sizeof(T) == 4 ? 2 : 15;  // the fastest one-step variant
     d->plan1 = le2d::plan_fused<T>(d->nx, d->ny, v, le2d::fused_resident_warps<T>(dev, v), kMinSeg);

@@ -37,8 +37,9 @@ int fused_variant_lanes(int variant);
 template <typename T>
 int fused_variant_depth(int variant);
 
+// halves: the task launches in halves (segment length fitted for that schedule).
 template <typename T>
-FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_seg);
+FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_seg, bool halves = false);
 
 // Warps of the fused kernel variant that fit on the device at once.
 template <typename T>

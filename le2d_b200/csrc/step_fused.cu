@@ -349,6 +349,11 @@ constexpr int kWaves = 8;
 //   each of those grids (an earlier fit without the length term: up to 7 % below it, e.g.
 //   147.4 against 158.3 Gnu/s on 3000^2, 155.1 against 158.4 on 4096^2; the earlier rule of
 //   about 8 waves of tiles: up to 13 % below it);
+//   warp-pair variants launched in halves (le2d_api.cu), w counting the tiles of one half:
+//   h = 14, beta = 0, alpha = 0.2, kappa = 0 -- fitted on the same grids with the halves
+//   forced on, it picks the fastest measured length, and the halves with it beat the best
+//   whole launches on each of those grids but 2048^2 (2 % below): e.g. 4096^2 176.2 against
+//   158.5, 8192 x 2048 179.5 against 158.7, 8192^2 195.2 against 181.8 Gnu/s;
 //   FP64 one-step variants, the FP64 default measured on 2048^2 to 12000^2 and 8192 x 2048
 //   with segments of 16 to 128 rows: h = 8, beta = 0.3, alpha = 0, kappa = 0.1 -- within 1 %
 //   of the fastest measured length on each (the 8-wave rule: up to 10 % below it, e.g. 40.3
@@ -361,6 +366,7 @@ struct SegModel {
 constexpr int kPairLens[] = {32, 48, 64, 80, 96, 128, 160, 192, 256};
 constexpr int kStepLensF64[] = {16, 24, 32, 40, 48, 56, 64, 80, 96, 112, 128};
 constexpr SegModel kPairModel{10.0, 0.1, 0.5, 0.02, kPairLens, 9};
+constexpr SegModel kPairHalvesModel{14.0, 0.0, 0.2, 0.0, kPairLens, 9};
 constexpr SegModel kStepModelF64{8.0, 0.3, 0.0, 0.1, kStepLensF64, 11};
 
 inline int model_segment(const SegModel& m, int ny, int nstrips, int resident_tiles, int min_len) {
@@ -381,7 +387,7 @@ inline int model_segment(const SegModel& m, int ny, int nstrips, int resident_ti
 }
 
 template <typename T>
-FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_seg) {
+FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_seg, bool halves) {
   FusedPlan pl;
   pl.variant = variant < 0 || variant >= kVariants ? 0 : variant;
   pl.lanes = fused_variant_lanes<T>(pl.variant);
@@ -394,7 +400,9 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
   if (target < 1) target = 1;
   int seg = (ny + target - 1) / target;
   if (seg < min_seg * pl.depth) seg = min_seg * pl.depth;
-  if (resident_tasks > 0 && pl.warps_per_task == 2)
+  if (resident_tasks > 0 && pl.warps_per_task == 2 && halves)  // each half's waves
+    seg = model_segment(kPairHalvesModel, ny, pl.nstrips, 2 * resident_tasks, min_seg * pl.depth);
+  else if (resident_tasks > 0 && pl.warps_per_task == 2)
     seg = model_segment(kPairModel, ny, pl.nstrips, resident_tasks, min_seg * pl.depth);
   else if (resident_tasks > 0 && sizeof(T) == 8 && pl.depth == 1)
     seg = model_segment(kStepModelF64, ny, pl.nstrips, resident_tasks, min_seg);
@@ -486,7 +494,7 @@ unsigned long long check_violations_fused() {
   template int fused_variant_lanes<T>(int);                                                     \
   template int fused_variant_depth<T>(int);                                                     \
   template int fused_resident_warps<T>(int, int);                                               \
-  template FusedPlan plan_fused<T>(int, int, int, int, int);                                    \
+  template FusedPlan plan_fused<T>(int, int, int, int, int, bool);                              \
   template cudaError_t launch_fused_step<T>(const T*, T*, int, int, long long, long long,       \
                                             const StepConsts<T>&, int, const FusedPlan&,        \
                                             const PairCtl&, cudaStream_t);                      \
