@@ -357,7 +357,10 @@ constexpr int kWaves = 8;
 //   FP64 one-step variants, the FP64 default measured on 2048^2 to 12000^2 and 8192 x 2048
 //   with segments of 16 to 128 rows: h = 8, beta = 0.3, alpha = 0, kappa = 0.1 -- within 1 %
 //   of the fastest measured length on each (the 8-wave rule: up to 10 % below it, e.g. 40.3
-//   against 44.2 Gnu/s on 2048^2, 46.6 against 51.3 on 4096^2).
+//   against 44.2 Gnu/s on 2048^2, 46.6 against 51.3 on 4096^2); launched in halves, with the
+//   waves of one half, h = 8, beta = 0, alpha = 0.2, kappa = 0.1 -- the fastest measured length
+//   on each (2-3 % above the whole launches' lengths in halves: 8192^2 58.8 against 57.3,
+//   2048^2 48.1 against 46.5 Gnu/s).
 struct SegModel {
   double h, beta, alpha, kappa;
   const int* lens;
@@ -368,6 +371,8 @@ constexpr int kStepLensF64[] = {16, 24, 32, 40, 48, 56, 64, 80, 96, 112, 128};
 constexpr SegModel kPairModel{10.0, 0.1, 0.5, 0.02, kPairLens, 9};
 constexpr SegModel kPairHalvesModel{14.0, 0.0, 0.2, 0.0, kPairLens, 9};
 constexpr SegModel kStepModelF64{8.0, 0.3, 0.0, 0.1, kStepLensF64, 11};
+constexpr int kStepHalvesLensF64[] = {16, 24, 32, 48, 64, 96, 128};
+constexpr SegModel kStepHalvesModelF64{8.0, 0.0, 0.2, 0.1, kStepHalvesLensF64, 7};
 
 inline int model_segment(const SegModel& m, int ny, int nstrips, int resident_tiles, int min_len) {
   int best_len = min_len < ny ? min_len : ny;
@@ -404,6 +409,8 @@ FusedPlan plan_fused(int nx, int ny, int variant, int resident_warps, int min_se
     seg = model_segment(kPairHalvesModel, ny, pl.nstrips, 2 * resident_tasks, min_seg * pl.depth);
   else if (resident_tasks > 0 && pl.warps_per_task == 2)
     seg = model_segment(kPairModel, ny, pl.nstrips, resident_tasks, min_seg * pl.depth);
+  else if (resident_tasks > 0 && sizeof(T) == 8 && pl.depth == 1 && halves)
+    seg = model_segment(kStepHalvesModelF64, ny, pl.nstrips, 2 * resident_tasks, min_seg);
   else if (resident_tasks > 0 && sizeof(T) == 8 && pl.depth == 1)
     seg = model_segment(kStepModelF64, ny, pl.nstrips, resident_tasks, min_seg);
   if (seg > ny) seg = ny;
