@@ -16,7 +16,10 @@ Our arm (default) prints one JSON line with
   roofline  the fused step kernel against the measured HBM copy bandwidth,
             40 algorithmic bytes per node-update in FP32 (read + write of 5 fields);
             a launch of temporal-block depth 2 advances every node two steps, so its
-            algorithmic bytes are 2 x 40 B per node while it moves about half of that,
+            algorithmic bytes are 2 x 40 B per node while it moves about half of that;
+            an update of the grid launched in halves (launch_parts 3: the band around the
+            middle row and the rows above and below it, overlapping) is timed as one launch,
+            and gpu_launches counts its 3 kernel launches,
   cpu_baseline  the reference's own simple/ solver (oracle/_ref) on the host cores,
   fp64      the same measurement for the FP64 library (80 B per node-update),
   batched   256 uneven FP32 solves (sides 128-2048, steps 200-2000) in the persistent
