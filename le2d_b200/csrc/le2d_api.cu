@@ -103,11 +103,10 @@ constexpr int kMinHalvesRows = 256;  // grids with fewer rows launch whole
 // 53.7, 8192^2 55.9 / 57.2.  LE2D_HALVES=1 / 0 overrides it (on every grid of at least
 // 4 kBand rows / never).
 bool halves_for(int ny) {
-  static int mode = -2;
-  if (mode == -2) {
+  static const int mode = [] {  // read once, thread-safely
     const char* e = getenv("LE2D_HALVES");
-    mode = e ? (atoi(e) != 0 ? 1 : 0) : -1;
-  }
+    return e ? (atoi(e) != 0 ? 1 : 0) : -1;
+  }();
   if (mode == 0 || ny < 4 * kBand) return false;
   return mode == 1 || ny >= kMinHalvesRows;
 }
@@ -184,12 +183,12 @@ std::mutex g_mu;
 std::unordered_map<const void*, DevTask*> g_tasks;
 
 int device_count() {
-  static int n = -1;
-  if (n < 0) {
+  static const int n = [] {  // queried once, thread-safely
     int c = 0;
-    n = cudaGetDeviceCount(&c) == cudaSuccess ? c : 0;
-    if (n == 0) cudaGetLastError();
-  }
+    const int k = cudaGetDeviceCount(&c) == cudaSuccess ? c : 0;
+    if (k == 0) cudaGetLastError();
+    return k;
+  }();
   return n;
 }
 
@@ -218,13 +217,12 @@ long long row_pitch(int nx) { return le2d::row_pitch_elems(nx); }
 // first, interior tiles on the lean one-step loop in 128 registers, 16 warps per SM -- the
 // FP64 two-step variants measured slower).
 int default_variant() {
-  static int v = -2;
-  if (v == -2) {
+  static const int v = [] {  // read once, thread-safely
     const int dflt = sizeof(T) == 4 ? 13 : 15;
     const char* e = getenv("LE2D_FUSED_VARIANT");
-    v = e ? atoi(e) : dflt;
-    if (v < 0 || v >= le2d::fused_variant_count<T>()) v = dflt;
-  }
+    const int x = e ? atoi(e) : dflt;
+    return x < 0 || x >= le2d::fused_variant_count<T>() ? dflt : x;
+  }();
   return v;
 }
 
